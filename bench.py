@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: masked-SpGEMM triangle counting on one B200 (and replicas).
+
+Default workload: triangle counting C<L> = L·L (plus-pair, sum of C) on the
+seeded RMAT scale-24 graph (16,777,216 vertices, edge factor 16,
+a/b/c/d = .57/.19/.19/.05, seed 5), L = strict lower triangle with int64 row
+pointers and int32 columns, device-resident.  A "step" is one gk_tc_count
+call over L (plan + binned kernels + fused sum).  Other workloads
+(--workload tc14 | ktruss20 | bc18) measure the other configurations.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU code (the GraphKokkos headers
+compiled against the Kokkos-API shim, oracle/_ref) on this host's cores on a
+bounded row sample of the same graph, same metric.
+Multi-GPU (torchrun): every rank runs an independent replica (the path has
+no exchange step); value = all ranks' edges / max time over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "masked-SpGEMM edges/s (TC, k-truss), BC TEPS; learned vs plain sched, 1 B200"
+MODEL_PATH = os.path.join(ROOT, "graphkokkos_b200", "sched", "model.npz")
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+WORKLOADS = {
+    "tc24": dict(kind="tc", scale=24, seed=5),
+    "tc20": dict(kind="tc", scale=20, seed=2),
+    "tc14": dict(kind="tc", scale=14, seed=1),
+    "ktruss20": dict(kind="ktruss", scale=20, seed=2, k=5),
+    "bc18": dict(kind="bc", scale=18, seed=3, nsrc=512, src_seed=4),
+}
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 f".clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def load_model(gk):
+    if not os.path.exists(MODEL_PATH):
+        return False
+    from graphkokkos_b200 import sched
+    sched.load_model(MODEL_PATH)
+    return True
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def time_steps(torch, fn, steps, warmup, dist=None):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    s = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    return e0.elapsed_time(e1) / steps
+
+
+def tc_roofline(gk, torch, L, sched, peak, peak_kind):
+    """Per-variant CUDA-event durations of one profiled call (work totals)
+    plus events-only brackets over timed calls; the dominant variant's
+    algorithmic bytes per launch divided by its mean launch time."""
+    lib = gk.load()
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    lib.gk_prof_enable(1)
+    gk.tc_count_device(L, out, sched=sched)
+    torch.cuda.synchronize()
+    work = {}
+    rec = gk._lib.GkProfRec()
+    for i in range(lib.gk_prof_count()):
+        lib.gk_prof_get(i, ctypes.byref(rec))
+        work[rec.variant] = (rec.rows, rec.sum_a, rec.sum_m, rec.sum_work)
+    lib.gk_prof_enable(2)
+    for _ in range(3):
+        gk.tc_count_device(L, out, sched=sched)
+    lib.gk_prof_flush()
+    times = {}
+    for i in range(lib.gk_prof_count()):
+        lib.gk_prof_get(i, ctypes.byref(rec))
+        times.setdefault(rec.variant, []).append(rec.ms)
+    lib.gk_prof_enable(0)
+    per = {}
+    for v, ts in times.items():
+        rows, sa, sm, sw = work.get(v, (0, 0, 0, 0))
+        # algorithmic bytes of the rows this variant ran (formula of the
+        # reference Gustavson formulation, RP = 8): B-row column stream 4·W,
+        # the L entries once 4·nnz, two row pointers per A entry and per row
+        alg = 4 * sw + 4 * sa + 16 * sa + 16 * rows
+        per[v] = dict(ms=float(np.mean(ts)), bytes=alg, rows=rows, work=sw)
+    dom = max(per, key=lambda v: per[v]["ms"])
+    d = per[dom]
+    achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
+    return {"kernel": f"masked SpGEMM variant {dom}", "bound": "hbm", "achieved": round(achieved, 1),
+            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic_for(dom), "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
+            "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "rows": x["rows"]}
+                         for v, x in sorted(per.items())}}
+
+
+def traffic_for(variant):
+    path = os.path.join(ROOT, "profiles", "tc_rmat24_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(str(variant))
+    except Exception:
+        return None
+
+
+def cpu_baseline(L_host, target_s=12.0):
+    """The reference's mxmm_msa (oracle/_ref, via the Kokkos-API shim) on a
+    strided row sample of L, on this host's cores; falls back to the port."""
+    import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    stride = 4096
+    cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
+    # grow the sample toward ~target_s seconds of CPU work
+    if sec > 0:
+        want = max(1, int(stride * sec / target_s))
+        stride = max(16, min(stride, want))
+        if stride < 4096:
+            cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
+    return {"value": nz / sec if sec > 0 else None, "unit": "edges/s", "cores": thr, "kind": kind,
+            "sample": f"rows i % {stride} == 0 of L ({nz} of {L_host.nnz} entries), {sec:.1f} s, "
+                      f"C<S> = S·L then sum (reference bracket src/main.cpp:74-85)"}
+
+
+def run_tc(args, wl, torch, gk, dist, rank, world):
+    scale, seed = wl["scale"], wl["seed"]
+    A = gk.gen_rmat(scale, 16, seed=seed, device="cuda")
+    L = gk.extract_lower(A)
+    del A
+    torch.cuda.empty_cache()
+    have_model = load_model(gk)
+    scheds = ["plain"] + (["learned"] if have_model else [])
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    lib = gk.load()
+    res = {}
+    count = None
+    for sched in scheds:
+        fn = lambda: gk.tc_count_device(L, out, sched=sched)  # noqa: E731
+        if sched == scheds[-1]:
+            clocks = ClockSampler(torch.cuda.current_device())
+            clocks.start()
+            l0 = lib.gk_launch_count()
+        ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+        if sched == scheds[-1]:
+            launches = lib.gk_launch_count() - l0
+            clk = clocks.stop()
+        c = int(out.item())
+        assert count is None or c == count, "schedulers disagree"
+        count = c
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res[sched] = {"value": L.nnz * world / (ms_max / 1e3), "ms_per_step": ms_max}
+    head = scheds[-1]
+    line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: seeded RMAT (a,b,c,d=.57,.19,.19,.05, edge factor 16, no noise/permutation), "
+                    "symmetrised, self-loops and duplicates removed, generated on the device",
+            "config": {"workload": f"triangle counting C<L>=L·L on RMAT-{scale} seed {seed}",
+                       "scale": scale, "edge_factor": 16, "seed": seed, "vertices": L.m, "nnz_lower": L.nnz,
+                       "rowptr": "int64", "sched": head, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": f"inputs larger than L2 (L = {L.nnz * 4 / 1e9:.2f} GB of columns, no flush needed)"},
+            "triangles": count, "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        line["roofline"] = tc_roofline(gk, torch, L, head, peak, peak_kind)
+        # end to end through the public API with host buffers: the H2D copy of
+        # L (pinned) and the D2H read of the count are inside the timed region
+        Lh = L.to("cpu")
+        Lh.rowptr = Lh.rowptr.pin_memory()
+        Lh.col = Lh.col.pin_memory()
+        e2e_steps = max(1, min(args.steps, 5))
+        gk.tc_count(Lh, sched=head)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            c = gk.tc_count(Lh, sched=head)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        assert c == count
+        line["e2e"] = {"value": L.nnz / e2e_s, "unit": "edges/s", "ms_per_step": e2e_s * 1e3,
+                       "h2d_bytes_per_step": 8 * (L.m + 1) + 4 * L.nnz, "d2h_bytes_per_step": 8,
+                       "api": "gk_tc_count with pinned host CSR arrays"}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(Lh.numpy())
+    return line
+
+
+def run_ktruss(args, wl, torch, gk, dist, rank, world):
+    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
+    iters = [0]
+
+    def fn():
+        T, it = gk.ktruss(A, wl["k"])
+        iters[0] = it
+    ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+    edges = A.nnz // 2
+    return {"metric": METRIC, "value": edges * world / (ms / 1e3), "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic: seeded RMAT",
+            "config": {"workload": f"k-truss k={wl['k']} on RMAT-{wl['scale']} seed {wl['seed']}",
+                       "iterations": iters[0], "edges": edges}}
+
+
+def run_bc(args, wl, torch, gk, dist, rank, world):
+    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
+    rng = np.random.default_rng(wl["src_seed"])
+    src = rng.choice(A.m, size=wl["nsrc"], replace=False)
+    out = [None]
+
+    def fn():
+        out[0] = gk.bc_batch(A, src)
+    ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+    # TEPS: undirected edges in each source's component
+    import scipy.sparse as sp
+    import scipy.sparse.csgraph as cg
+    rp = A.rowptr.cpu().numpy()
+    col = A.col.cpu().numpy()
+    M = sp.csr_matrix((np.ones(len(col), dtype=np.int8), col, rp), shape=(A.m, A.m))
+    ncomp, lab = cg.connected_components(M, directed=False)
+    edges_per_comp = np.bincount(lab[np.repeat(np.arange(A.m), np.diff(rp))], minlength=ncomp) // 2
+    traversed = int(edges_per_comp[lab[src]].sum())
+    return {"metric": METRIC, "value": traversed * world / (ms / 1e3), "unit": "TEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded RMAT",
+            "config": {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources",
+                       "teps_all_edges": (A.nnz // 2) * len(src) / (ms / 1e3)}}
+
+
+def main_ours(args):
+    import torch
+    rank, local, world = rank_info()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    else:
+        torch.cuda.set_device(0)
+    import graphkokkos_b200 as gk
+    gk.load()
+    wl = WORKLOADS[args.workload]
+    runner = {"tc": run_tc, "ktruss": run_ktruss, "bc": run_bc}[wl["kind"]]
+    line = runner(args, wl, torch, gk, dist, rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU code on this host's cores
+# ---------------------------------------------------------------------------
+def main_reference(args):
+    rank, _, world = rank_info()
+    if rank != 0:
+        return
+    import oracle
+    import graphkokkos_b200 as gk
+    wl = WORKLOADS[args.workload]
+    if wl["kind"] != "tc":
+        print(json.dumps({"impl": "reference", "unavailable": "reference arm implemented for the tc workloads"}))
+        return
+    try:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+    except Exception:
+        dev = "cpu"
+    # input generation is not timed; the GPU builder is used when present
+    if dev == "cuda":
+        A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
+        L = gk.extract_lower(A).numpy()
+        del A
+    else:
+        L = gk.lower_host(gk.gen_rmat(wl["scale"], 16, seed=wl["seed"]))
+    kind = "reference" if oracle.ref_available() else "port"
+    # size the per-step sample so that warmup + steps stay within a few minutes
+    per_step_budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
+    stride = 1 << 14
+    _, nz, sec, thr = oracle.tc_row_stride(L, stride, 0, kind=kind)
+    if sec > 0:
+        stride = max(1, min(stride, int(stride * sec / per_step_budget)))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cnt, nz, sec, thr = oracle.tc_row_stride(L, stride, i % stride, kind=kind)
+        if i >= args.warmup:
+            vals.append(nz / sec)
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic: seeded RMAT", "impl": "reference",
+            "config": {"workload": f"triangle counting C<L>=L·L on RMAT-{wl['scale']} seed {wl['seed']}",
+                       "scale": wl["scale"], "seed": wl["seed"], "nnz_lower": L.nnz},
+            "cpu_baseline": {"value": v, "unit": "edges/s", "cores": thr, "kind": kind,
+                             "sample": f"each step: rows i % {stride} == offset of L, reference mxmm_msa + sum"},
+            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tc24")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_ours(args)
+
+
+if __name__ == "__main__":
+    main()

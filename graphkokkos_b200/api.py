@@ -1,0 +1,302 @@
+"""Python host API over the C ABI (include/gk_b200.h).
+
+Mirrors the reference's operator surface (src/main.cpp:13-141,
+include/matrix_la.h:562-694, include/betweenness_centrality.h:406-506) with
+CSR matrices whose arrays are numpy arrays (host) or torch tensors (host or
+CUDA).  Every call goes to the CUDA library; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import GkCsr, GkCsrMut, check
+
+_SCHED = {"plain": _lib.GK_SCHED_PLAIN, "learned": _lib.GK_SCHED_LEARNED}
+_ACCUM = {"auto": _lib.GK_ACCUM_AUTO, "msa": _lib.GK_ACCUM_MSA, "mca": _lib.GK_ACCUM_MCA, "hash": _lib.GK_ACCUM_HASH}
+_SEMIRING = {"plus_times": _lib.GK_PLUS_TIMES, "plus_pair": _lib.GK_PLUS_PAIR}
+
+
+def _is_torch(x):
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor)
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        if not x.flags.c_contiguous:
+            raise ValueError("arrays must be contiguous")
+        return x.ctypes.data
+    if _is_torch(x):
+        if not x.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return x.data_ptr()
+    raise TypeError(f"unsupported array type {type(x)}")
+
+
+def _on_cuda(x):
+    return _is_torch(x) and x.is_cuda
+
+
+def _stream(stream, *arrays):
+    """cudaStream_t handle: the given one, else torch's current stream when the
+    arrays live on a CUDA device, else the legacy default stream."""
+    if stream is not None:
+        return ctypes.c_void_p(int(stream))
+    if any(_on_cuda(a) for a in arrays if a is not None):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(0)
+
+
+@dataclass
+class Csr:
+    """CSR matrix: spMtx<T> (include/matrix.h:33-43) with int64 row pointers."""
+
+    m: int
+    n: int
+    rowptr: object
+    col: object
+    val: object = None
+    nnz: Optional[int] = None
+
+    def __post_init__(self):
+        if self.nnz is None:
+            self.nnz = int(self.col.shape[0]) if self.col is not None else 0
+
+    def as_gk(self) -> GkCsr:
+        return GkCsr(self.m, self.n, self.nnz, _ptr(self.rowptr), _ptr(self.col), _ptr(self.val))
+
+    @property
+    def is_cuda(self):
+        return _on_cuda(self.rowptr)
+
+    def to(self, device):
+        """Copy to a torch device ("cuda", "cpu") or to numpy (device=None)."""
+        import torch
+
+        def conv(a):
+            if a is None:
+                return None
+            if device is None:
+                return a.cpu().numpy() if _is_torch(a) else a
+            t = torch.as_tensor(a) if not _is_torch(a) else a
+            return t.to(device)
+
+        return Csr(self.m, self.n, conv(self.rowptr), conv(self.col), conv(self.val), self.nnz)
+
+    def numpy(self):
+        return self.to(None)
+
+
+def _empty_like_space(ref, shape, dtype):
+    """An output array in the same memory space as `ref`."""
+    if _on_cuda(ref):
+        import torch
+        tdt = {np.int64: torch.int64, np.int32: torch.int32, np.uint64: torch.int64, np.float64: torch.float64,
+               np.float32: torch.float32}[dtype]
+        return torch.empty(shape, dtype=tdt, device=ref.device)
+    return np.empty(shape, dtype=dtype)
+
+
+# ---------------------------------------------------------------------------
+# masked SpGEMM family
+# ---------------------------------------------------------------------------
+def mxmm_masked(A: Csr, B: Csr, M: Csr, semiring="plus_times", sched="plain", accum="auto", out=None,
+                stream=None):
+    """C<M> = A·B; returns the nnz(M) values of C in M's pattern order
+    (mxmm_msa / mxmm_mca, include/matrix_la.h:478-694)."""
+    lib = _lib.load()
+    if out is None:
+        out = _empty_like_space(M.col, (M.nnz,), np.int32)
+    a, b, m = A.as_gk(), B.as_gk(), M.as_gk()
+    check(lib.gk_mxmm_masked(ctypes.byref(a), ctypes.byref(b), ctypes.byref(m), _ptr(out), _SEMIRING[semiring],
+                             _SCHED[sched], _ACCUM[accum], _stream(stream, M.col)))
+    return out
+
+
+def tc_count(L: Csr, sched="plain", stream=None) -> int:
+    """Triangle count from the strict lower triangle L (src/main.cpp:69-90)."""
+    lib = _lib.load()
+    out = ctypes.c_uint64(0)
+    g = L.as_gk()
+    check(lib.gk_tc_count(ctypes.byref(g), ctypes.addressof(out), _SCHED[sched], _stream(stream, L.col)))
+    return int(out.value)
+
+
+def tc_count_variant(L: Csr, variant: int, stream=None) -> int:
+    """Triangle count with every row on one kernel variant (tests, autotuner)."""
+    lib = _lib.load()
+    out = ctypes.c_uint64(0)
+    g = L.as_gk()
+    check(lib.gk_tc_count_variant(ctypes.byref(g), int(variant), ctypes.addressof(out), _stream(stream, L.col)))
+    return int(out.value)
+
+
+def mxmm_masked_variant(A: Csr, B: Csr, M: Csr, variant: int, semiring="plus_times", out=None, stream=None):
+    lib = _lib.load()
+    if out is None:
+        out = _empty_like_space(M.col, (M.nnz,), np.int32)
+    a, b, m = A.as_gk(), B.as_gk(), M.as_gk()
+    check(lib.gk_mxmm_masked_variant(ctypes.byref(a), ctypes.byref(b), ctypes.byref(m), _ptr(out),
+                                     _SEMIRING[semiring], int(variant), _stream(stream, M.col)))
+    return out
+
+
+def num_variants() -> int:
+    return int(_lib.load().gk_sched_num_variants())
+
+
+def tc_count_device(L: Csr, out, sched="plain", stream=None):
+    """Asynchronous variant: writes the count into a 1-element int64 CUDA tensor."""
+    lib = _lib.load()
+    g = L.as_gk()
+    check(lib.gk_tc_count(ctypes.byref(g), _ptr(out), _SCHED[sched], _stream(stream, L.col)))
+    return out
+
+
+def tc_row_sums(L: Csr, sched="plain", stream=None):
+    lib = _lib.load()
+    out = _empty_like_space(L.rowptr, (L.m,), np.uint64)
+    g = L.as_gk()
+    check(lib.gk_tc_row_sums(ctypes.byref(g), _ptr(out), _SCHED[sched], _stream(stream, L.col)))
+    return out
+
+
+def tc_count_batched(graphs: Sequence[Csr], sched="plain", stream=None):
+    lib = _lib.load()
+    n = len(graphs)
+    arr = (GkCsr * max(n, 1))(*[g.as_gk() for g in graphs])
+    out = np.zeros(n, dtype=np.uint64)
+    check(lib.gk_tc_count_batched(arr, n, out.ctypes.data, _SCHED[sched],
+                                  _stream(stream, *(g.col for g in graphs[:1]))))
+    return out
+
+
+def ktruss(A: Csr, k: int, sched="plain", stream=None):
+    """k-truss (src/main.cpp:94-141); returns (truss CSR, iterations)."""
+    lib = _lib.load()
+    if _is_torch(A.rowptr):
+        rp, col = A.rowptr.clone(), A.col.clone()
+    else:
+        rp, col = np.array(A.rowptr, copy=True), np.array(A.col, copy=True)
+    g = GkCsrMut(A.m, A.n, A.nnz, _ptr(rp), _ptr(col))
+    iters = ctypes.c_int(0)
+    check(lib.gk_ktruss(ctypes.byref(g), int(k), ctypes.byref(iters), _SCHED[sched], _stream(stream, A.col)))
+    nnz = int(g.nnz)
+    return Csr(A.m, A.n, rp, col[:nnz], None, nnz), int(iters.value)
+
+
+def bc_batch(A: Csr, sources, sched="plain", stream=None):
+    """FP64 batched betweenness centrality over `sources`
+    (include/betweenness_centrality.h:406-506)."""
+    lib = _lib.load()
+    if _on_cuda(A.rowptr):
+        import torch
+        src = torch.as_tensor(np.asarray(sources, dtype=np.int32)).to(A.rowptr.device)
+    else:
+        src = np.ascontiguousarray(np.asarray(sources, dtype=np.int32))
+    out = _empty_like_space(A.rowptr, (A.m,), np.float64)
+    g = A.as_gk()
+    check(lib.gk_bc_batch(ctypes.byref(g), _ptr(src), int(len(src)), _ptr(out), _SCHED[sched],
+                          _stream(stream, A.col)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CSR transforms
+# ---------------------------------------------------------------------------
+def extract_lower(A: Csr, stream=None) -> Csr:
+    lib = _lib.load()
+    rp = _empty_like_space(A.rowptr, (A.m + 1,), np.int64)
+    col = _empty_like_space(A.col, (max(A.nnz, 1),), np.int32)
+    nnz = ctypes.c_int64(0)
+    g = A.as_gk()
+    check(lib.gk_extract_lower(ctypes.byref(g), _ptr(rp), _ptr(col), ctypes.byref(nnz), _stream(stream, A.col)))
+    n = int(nnz.value)
+    return Csr(A.m, A.n, rp, col[:n], None, n)
+
+
+def transpose(A: Csr, with_values=False, stream=None) -> Csr:
+    lib = _lib.load()
+    rp = _empty_like_space(A.rowptr, (A.n + 1,), np.int64)
+    col = _empty_like_space(A.col, (max(A.nnz, 1),), np.int32)
+    val = _empty_like_space(A.col, (max(A.nnz, 1),), np.int32) if with_values else None
+    g = A.as_gk()
+    check(lib.gk_transpose(ctypes.byref(g), _ptr(rp), _ptr(col), _ptr(val), _stream(stream, A.col)))
+    return Csr(A.n, A.m, rp, col[:A.nnz], None if val is None else val[:A.nnz], A.nnz)
+
+
+# ---------------------------------------------------------------------------
+# graph generation
+# ---------------------------------------------------------------------------
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+def gen_rmat(scale, edge_factor=16, seed=1, abc=RMAT_ABC, device="cpu") -> Csr:
+    """Seeded RMAT graph (symmetric, no self-loops/duplicates, sorted rows).
+    device="cpu": host builder (numpy arrays); "cuda": device builder (torch)."""
+    lib = _lib.load()
+    m = 1 << scale
+    a, b, c = abc
+    if device == "cpu":
+        h = ctypes.c_void_p()
+        check(lib.gk_gen_rmat_host(scale, edge_factor, a, b, c, seed, ctypes.byref(h)))
+        return _take_host_graph(lib, h)
+    import torch
+    nnz = ctypes.c_int64(0)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib.gk_gen_rmat(scale, edge_factor, a, b, c, seed, ctypes.byref(nnz), None, None, s))
+    rp = torch.empty(m + 1, dtype=torch.int64, device=device)
+    col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=device)
+    check(lib.gk_gen_rmat(scale, edge_factor, a, b, c, seed, ctypes.byref(nnz), _ptr(rp), _ptr(col), s))
+    return Csr(m, m, rp, col[:nnz.value], None, int(nnz.value))
+
+
+def gen_er(n, nedges, seed=1, device="cpu") -> Csr:
+    lib = _lib.load()
+    if device == "cpu":
+        h = ctypes.c_void_p()
+        check(lib.gk_gen_er_host(n, nedges, seed, ctypes.byref(h)))
+        return _take_host_graph(lib, h)
+    import torch
+    nnz = ctypes.c_int64(0)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib.gk_gen_er(n, nedges, seed, ctypes.byref(nnz), None, None, s))
+    rp = torch.empty(n + 1, dtype=torch.int64, device=device)
+    col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=device)
+    check(lib.gk_gen_er(n, nedges, seed, ctypes.byref(nnz), _ptr(rp), _ptr(col), s))
+    return Csr(n, n, rp, col[:nnz.value], None, int(nnz.value))
+
+
+def _take_host_graph(lib, h) -> Csr:
+    m = ctypes.c_int64(0)
+    nnz = ctypes.c_int64(0)
+    lib.gk_host_graph_info(h, ctypes.byref(m), ctypes.byref(nnz))
+    rp = np.empty(m.value + 1, dtype=np.int64)
+    col = np.empty(nnz.value, dtype=np.int32)
+    lib.gk_host_graph_copy(h, rp.ctypes.data, col.ctypes.data if nnz.value else None)
+    lib.gk_host_graph_free(h)
+    return Csr(int(m.value), int(m.value), rp, col, None, int(nnz.value))
+
+
+def lower_host(A: Csr) -> Csr:
+    """Strict lower triangle of a host CSR with numpy (input preparation)."""
+    rp = np.asarray(A.rowptr)
+    col = np.asarray(A.col)
+    rows = np.repeat(np.arange(A.m, dtype=np.int64), np.diff(rp))
+    keep = col < rows
+    cnt = np.bincount(rows[keep], minlength=A.m)
+    lrp = np.zeros(A.m + 1, dtype=np.int64)
+    np.cumsum(cnt, out=lrp[1:])
+    lcol = np.ascontiguousarray(col[keep])
+    return Csr(A.m, A.n, lrp, lcol, None, int(lcol.shape[0]))

@@ -1,0 +1,110 @@
+// Common device/host utilities of the B200 library: status handling, the
+// device CSR view, stream-ordered scratch allocation and launch sizing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/gk_b200.h"
+
+namespace gk {
+
+// ----- status / last error ---------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define GK_CUDA(expr)                                  \
+    do {                                               \
+        cudaError_t _e = (expr);                       \
+        if (_e != cudaSuccess) return gk::cuda_fail(_e, #expr); \
+    } while (0)
+
+#define GK_CHECK(expr)                 \
+    do {                               \
+        int _s = (expr);               \
+        if (_s != GK_OK) return _s;    \
+    } while (0)
+
+// ----- device CSR view ---------------------------------------------------------
+struct DevCsr {
+    int64_t m, n, nnz;
+    const int64_t *rp;
+    const int32_t *col;
+    const int32_t *val;  // nullptr: every stored value is 1
+};
+
+// ----- per-device context ------------------------------------------------------
+struct Context {
+    int device = -1;
+    int num_sms = 0;
+    int max_smem_optin = 0;
+    bool pool_ready = false;
+};
+// Returns the context of the current device (created on first use).
+Context &ctx();
+
+// Stream-ordered scratch: a vector of allocations released together, in
+// stream order, when the guard goes out of scope.
+class Scratch {
+public:
+    explicit Scratch(cudaStream_t s) : stream_(s) {}
+    ~Scratch() { release(); }
+    Scratch(const Scratch &) = delete;
+    Scratch &operator=(const Scratch &) = delete;
+    // Allocates `bytes` (rounded up to 256) on the stream; returns GK_OK or an error code.
+    template <class T>
+    int alloc(T **out, size_t count) {
+        void *p = nullptr;
+        int s = raw_alloc(&p, count * sizeof(T));
+        *out = static_cast<T *>(p);
+        return s;
+    }
+    void release();
+
+private:
+    int raw_alloc(void **p, size_t bytes);
+    cudaStream_t stream_;
+    void *ptrs_[64] = {};
+    int n_ = 0;
+};
+
+// Host-or-device staging of a CSR: if the arrays are host memory they are
+// copied to HBM on the stream (into scratch), otherwise used in place.
+int stage_csr(const gk_csr *in, DevCsr *out, Scratch &scr, cudaStream_t s, int64_t *h2d_bytes = nullptr);
+bool is_device_pointer(const void *p);
+int validate_csr_shape(const gk_csr *c, const char *name);
+
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// ----- launch counter and per-variant profiling (gk_launch_count, gk_prof_*) ----
+void note_launches(int n);
+bool prof_enabled();
+
+struct ProfTotals {
+    unsigned long long rows, sum_a, sum_m, sum_work;
+};
+
+// Brackets kernel launches with CUDA events when profiling is on; finish()
+// synchronises the stream and appends one gk_prof_rec per bracketed slot.
+class ProfWindow {
+public:
+    ProfWindow(cudaStream_t s, int slots);
+    ~ProfWindow();
+    bool active() const { return on_; }
+    void begin(int slot);
+    void end(int slot);
+    int finish(const ProfTotals *totals);
+
+private:
+    cudaStream_t s_;
+    bool on_;
+    bool events_only_ = false;
+    int slots_;
+    cudaEvent_t ev_[64][2];
+    bool used_[64];
+};
+
+}  // namespace gk

@@ -1,0 +1,136 @@
+// Device-side building blocks of the masked SpGEMM kernels: thread-group
+// masks, shared-memory hash sets of mask columns, group-cooperative search in
+// sorted CSR rows, and reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gk {
+
+constexpr int EMPTY_KEY = -1;
+
+// Lanes of the calling thread's aligned group of G threads inside its warp.
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if constexpr (G >= 32) {
+        return 0xFFFFFFFFu;
+    } else {
+        const unsigned base = (threadIdx.x & 31) / G * G;
+        return ((1u << G) - 1u) << base;
+    }
+}
+
+template <int G>
+__device__ __forceinline__ unsigned low_bits() {
+    if constexpr (G >= 32) return 0xFFFFFFFFu;
+    else return (1u << G) - 1u;
+}
+
+// Multiplicative (Fibonacci) hashing of a column index into 2^LOG2 slots.
+template <int CAP>
+__device__ __forceinline__ int hash_slot(int x) {
+    constexpr int LOG2 = __builtin_ctz(CAP);
+    return static_cast<int>((static_cast<uint32_t>(x) * 0x9E3779B1u) >> (32 - LOG2));
+}
+
+// Inserts x into an open-addressing (linear probing) table; concurrent
+// inserts of distinct keys are safe.  The caller guarantees fewer than CAP
+// keys, so a free slot always exists; the probe count is bounded anyway.
+template <int CAP>
+__device__ __forceinline__ void hash_insert(int *keys, int x) {
+    int s = hash_slot<CAP>(x);
+#pragma unroll 1
+    for (int probe = 0; probe < CAP; ++probe) {
+        const int prev = atomicCAS(keys + s, EMPTY_KEY, x);
+        if (prev == EMPTY_KEY || prev == x) return;
+        s = (s + 1) & (CAP - 1);
+    }
+}
+
+// Slot of x, or -1 when x is not a key.
+template <int CAP>
+__device__ __forceinline__ int hash_find(const int *keys, int x) {
+    int s = hash_slot<CAP>(x);
+#pragma unroll 1
+    for (int probe = 0; probe < CAP; ++probe) {
+        const int k = keys[s];
+        if (k == x) return s;
+        if (k == EMPTY_KEY) return -1;
+        s = (s + 1) & (CAP - 1);
+    }
+    return -1;
+}
+
+// Index of x in sorted keys[0, n), or -1.
+__device__ __forceinline__ int sorted_find(const int *keys, int n, int x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && keys[lo] == x) ? lo : -1;
+}
+
+// First index in [lo, hi) with a[idx] >= x, for a sorted ascending; computed
+// cooperatively by the G lanes of a group (a G-ary search: every round each
+// lane probes one pivot, a ballot counts the pivots below x).  All lanes of
+// the group must call it with the same arguments; all get the result.
+template <int G>
+__device__ __forceinline__ int64_t group_lower_bound(const int32_t *__restrict__ a, int64_t lo, int64_t hi,
+                                                     int x, int lane, unsigned gmask) {
+    const unsigned shift = (G >= 32) ? 0u : ((threadIdx.x & 31) / G * G);
+#pragma unroll 1
+    while (hi - lo > G) {
+        const int64_t len = hi - lo;
+        const int64_t piv = lo + (len * (lane + 1)) / (G + 1);
+        const bool below = a[piv] < x;
+        const unsigned bal = (__ballot_sync(gmask, below) >> shift) & low_bits<G>();
+        const int c = __popc(bal);
+        const int64_t new_lo = (c == 0) ? lo : lo + (len * c) / (G + 1) + 1;
+        const int64_t new_hi = (c == G) ? hi : lo + (len * (c + 1)) / (G + 1);
+        lo = new_lo;
+        hi = new_hi;
+    }
+    const bool below = (lo + lane < hi) && a[lo + lane] < x;
+    const unsigned bal = (__ballot_sync(gmask, below) >> shift) & low_bits<G>();
+    return lo + __popc(bal);
+}
+
+// Sum over the G lanes of a group (all lanes get the total).
+template <int G, class T>
+__device__ __forceinline__ T group_sum(T v, unsigned gmask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o, G);
+    return v;
+}
+
+// Block-wide sum; every thread of the block must call it.  Result valid in
+// thread 0.  `red` is shared scratch of at least blockDim.x/32 entries.
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T *red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+    return t;
+}
+
+__device__ __forceinline__ int ilog2_u64(unsigned long long x) { return x ? 63 - __clzll(x) : 0; }
+
+// Number of A-entry splits of a row in the block kinds.
+__host__ __device__ __forceinline__ int64_t num_splits(int64_t work, int64_t a_len, int split_log2) {
+    if (split_log2 <= 0 || a_len <= 1) return 1;
+    int64_t s = (work + (int64_t(1) << split_log2) - 1) >> split_log2;
+    if (s < 1) s = 1;
+    if (s > a_len) s = a_len;
+    if (s > 4096) s = 4096;
+    return s;
+}
+
+}  // namespace gk

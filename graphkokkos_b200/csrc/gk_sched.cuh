@@ -1,0 +1,81 @@
+// Row binning and kernel-variant catalog of the masked SpGEMM engine.
+//
+// The reference's only scheduling is a choice of accumulator per call
+// (src/main.cpp:194-212) and an nnz-balanced split of rows over threads
+// (matrix_la.h:590-596).  Here every row of C<M> = A·B is placed in a bin by
+// two features — the mask-row length nnz(M_i) and the mean length of the B
+// rows it streams, work_i / nnz(A_i) with work_i = sum_{k in A_i} nnz(B_k) —
+// and each bin is assigned one kernel variant (accumulator family, threads
+// per row, mask-chunk capacity, work per item) by either the plain heuristic
+// or the learned MLP.  The variant only decides how a row is computed, never
+// what: all variants accumulate the same integer terms.
+#pragma once
+#include <stdint.h>
+
+namespace gk {
+
+// ---- bins -------------------------------------------------------------------
+constexpr int NB_M = 16;  // floor(log2(nnz(M_i))), capped
+constexpr int NB_B = 16;  // floor(log2(mean nnz(B_k))), capped
+constexpr int NBINS = NB_M * NB_B;
+constexpr uint16_t BIN_SKIP = 0xFFFF;  // row with no work or an empty mask row
+
+struct BinStats {
+    unsigned long long rows;
+    unsigned long long sum_m;     // sum of nnz(M_i)
+    unsigned long long sum_a;     // sum of nnz(A_i)
+    unsigned long long sum_work;  // sum of work_i
+    unsigned int max_b;           // max nnz(B_k) seen by any row of the bin
+    unsigned int pad;
+};
+
+// ---- variants -----------------------------------------------------------------
+enum Kind : int { K_HASH_GROUP = 0, K_HASH_BLOCK = 1, K_MCA_GROUP = 2, K_MCA_BLOCK = 3, K_MSA_BLOCK = 4 };
+
+struct Variant {
+    int kind;
+    int G;          // threads per row (group kinds) or per CTA (block kinds)
+    int cap;        // hash slots (HASH), sorted slots (MCA), log2 window columns (MSA)
+    int cap_write;  // same when values are written back (WRITE epilogue needs accumulators)
+    int chunk;      // mask entries per item (HASH/MCA); unused by MSA
+    int chunk_write;
+    int split_log2; // block kinds: work per item before a row's A entries are split
+    int accum;      // gk_accum family this variant belongs to
+};
+
+constexpr int NV = 10;
+// Shared-memory budget of every variant is below 160 KB; see the kernels.
+// columns: kind, G, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, accum family
+#define GK_VARIANT_TABLE { \
+    {K_HASH_GROUP,   4,    64,    64,    16,    16,   0, 3},   \
+    {K_HASH_GROUP,   8,   128,   128,    32,    32,   0, 3},   \
+    {K_HASH_GROUP,  16,   256,   256,    64,    64,   0, 3},   \
+    {K_HASH_GROUP,  32,   512,   512,   128,   128,   0, 3},   \
+    {K_HASH_GROUP,  32,  2048,  2048,   512,   512,   0, 3},   \
+    {K_HASH_BLOCK, 256,  8192,  8192,  4096,  4096,  20, 3},   \
+    {K_HASH_BLOCK, 512, 32768, 16384, 16384,  8192,  22, 3},   \
+    {K_MCA_GROUP,   32,   256,   256,   256,   256,   0, 2},   \
+    {K_MCA_BLOCK,  512, 16384, 16384, 16384, 16384,  22, 2},   \
+    {K_MSA_BLOCK,  512,    20,    15,     0,     0,  22, 1},   \
+}
+constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
+#ifdef __CUDACC__
+__constant__ const Variant c_variants[NV] = GK_VARIANT_TABLE;  // runtime-indexed copy for device code
+#endif
+constexpr int NT_GROUP = 256;  // CTA size of the group kinds (variant 4 uses 128)
+__host__ __device__ constexpr int group_cta_threads(int v) { return v == 4 ? 128 : NT_GROUP; }
+
+// ---- features of a bin (inputs of the learned scheduler) ---------------------
+constexpr int NFEAT = 8;
+// f0 log2(1+mean nnz(M_i))   f1 log2(1+mean nnz(B_k))   f2 log2(1+mean nnz(A_i))
+// f3 log2(1+mean work_i)     f4 log2(1+max nnz(B_k)) - f1 (degree skew)
+// f5 log2(1+rows)            f6 1 if values are written back (WRITE epilogue)
+// f7 1 if A or B carries values (plus-times) else 0 (plus-pair)
+
+// ---- MLP of the learned scheduler --------------------------------------------
+constexpr int MLP_H = 32;
+// layout (float32): W1[MLP_H][NFEAT], b1[MLP_H], W2[MLP_H][MLP_H], b2[MLP_H],
+//                   W3[NV][MLP_H], b3[NV], mu[NFEAT], sigma[NFEAT]
+constexpr int MLP_SIZE = MLP_H * NFEAT + MLP_H + MLP_H * MLP_H + MLP_H + NV * MLP_H + NV + 2 * NFEAT;
+
+}  // namespace gk

@@ -1,0 +1,170 @@
+// Row-bin scheduler of the masked SpGEMM engine: the plain binning
+// heuristic and the learned MLP (inference on the device), plus the model
+// registry behind gk_sched_set_model.
+//
+// No reference counterpart beyond the CLI's per-call accumulator choice
+// (src/main.cpp:194-212).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "gk_common.cuh"
+#include "gk_sched.cuh"
+#include "gk_spgemm.cuh"
+
+namespace gk {
+
+__device__ float d_mlp[MLP_SIZE];
+
+static std::mutex g_model_mutex;
+static std::vector<float> g_model;     // host copy
+static int g_model_version = 0;
+static int g_model_uploaded[64];       // version uploaded per device
+
+__host__ __device__ inline void bin_features(const BinStats &b, int epi, bool values, float *f) {
+    const double rows = static_cast<double>(b.rows);
+    const double mean_m = b.sum_m / rows;
+    const double mean_b = b.sum_a ? static_cast<double>(b.sum_work) / static_cast<double>(b.sum_a) : 0.0;
+    const double mean_a = b.sum_a / rows;
+    const double mean_w = b.sum_work / rows;
+    f[0] = static_cast<float>(log2(1.0 + mean_m));
+    f[1] = static_cast<float>(log2(1.0 + mean_b));
+    f[2] = static_cast<float>(log2(1.0 + mean_a));
+    f[3] = static_cast<float>(log2(1.0 + mean_w));
+    f[4] = static_cast<float>(log2(1.0 + static_cast<double>(b.max_b))) - f[1];
+    f[5] = static_cast<float>(log2(1.0 + rows));
+    f[6] = epi == EPI_WRITE ? 1.0f : 0.0f;
+    f[7] = values ? 1.0f : 0.0f;
+}
+
+// Plain heuristic: the smallest structure that holds the mask row in one
+// chunk, a wider thread group when the streamed B rows are long, and a block
+// kind (which splits rows over CTAs) when a row carries a lot of work.
+__host__ __device__ inline int plain_variant(int bin, const BinStats &b) {
+    const int qm = bin / NB_B, qb = bin % NB_B;
+    int v;
+    if (qm <= 3) v = 0;
+    else if (qm == 4) v = 1;
+    else if (qm == 5) v = 2;
+    else if (qm == 6) v = 3;
+    else if (qm <= 8) v = 4;
+    else if (qm <= 11) v = 5;
+    else v = 6;
+    if (v <= 1 && qb >= 4) v = 2;
+    if (v <= 2 && qb >= 6) v = 3;
+    const double mean_w = static_cast<double>(b.sum_work) / static_cast<double>(b.rows ? b.rows : 1);
+    if (v <= 4 && mean_w > double(1 << 21)) v = 5;
+    return v;
+}
+
+__host__ __device__ inline int forced_variant(int bin, const BinStats &b, int accum) {
+    const int qm = bin / NB_B;
+    switch (accum) {
+        case GK_ACCUM_MSA: return 9;
+        case GK_ACCUM_MCA: return qm <= 7 ? 7 : 8;
+        default: return plain_variant(bin, b);
+    }
+}
+
+__device__ inline int mlp_variant(const float *w, const float *f_raw) {
+    const float *W1 = w;
+    const float *b1 = W1 + MLP_H * NFEAT;
+    const float *W2 = b1 + MLP_H;
+    const float *b2 = W2 + MLP_H * MLP_H;
+    const float *W3 = b2 + MLP_H;
+    const float *b3 = W3 + NV * MLP_H;
+    const float *mu = b3 + NV;
+    const float *sg = mu + NFEAT;
+    float x[NFEAT], h1[MLP_H], h2[MLP_H];
+    for (int i = 0; i < NFEAT; ++i) x[i] = (f_raw[i] - mu[i]) / sg[i];
+    for (int j = 0; j < MLP_H; ++j) {
+        float a = b1[j];
+        for (int i = 0; i < NFEAT; ++i) a += W1[j * NFEAT + i] * x[i];
+        h1[j] = a > 0.f ? a : 0.f;
+    }
+    for (int j = 0; j < MLP_H; ++j) {
+        float a = b2[j];
+        for (int i = 0; i < MLP_H; ++i) a += W2[j * MLP_H + i] * h1[i];
+        h2[j] = a > 0.f ? a : 0.f;
+    }
+    int best = 0;
+    float best_s = 3.0e38f;
+    for (int v = 0; v < NV; ++v) {
+        float a = b3[v];
+        for (int i = 0; i < MLP_H; ++i) a += W3[v * MLP_H + i] * h2[i];
+        if (a < best_s) {
+            best_s = a;
+            best = v;
+        }
+    }
+    return best;
+}
+
+__global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int accum, int epi, bool values) {
+    const int b = threadIdx.x + blockIdx.x * blockDim.x;
+    if (b >= NBINS) return;
+    const BinStats st = bins[b];
+    if (st.rows == 0) {
+        var_of_bin[b] = 0;
+        return;
+    }
+    int v;
+    if (accum != GK_ACCUM_AUTO) v = forced_variant(b, st, accum);
+    else if (mode == GK_SCHED_LEARNED) {
+        float f[NFEAT];
+        bin_features(st, epi, values, f);
+        v = mlp_variant(d_mlp, f);
+    } else v = plain_variant(b, st);
+    var_of_bin[b] = v;
+}
+
+static int ensure_model_on_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_model_mutex);
+    if (g_model.empty()) return fail(GK_ERR_ARG, "learned scheduler requested but no model is loaded (gk_sched_set_model)");
+    if (g_model_uploaded[dev & 63] != g_model_version) {
+        GK_CUDA(cudaMemcpyToSymbol(d_mlp, g_model.data(), sizeof(float) * MLP_SIZE));
+        g_model_uploaded[dev & 63] = g_model_version;
+    }
+    return GK_OK;
+}
+
+int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_accum, int epi, bool values,
+                 cudaStream_t s) {
+    if (sched != GK_SCHED_PLAIN && sched != GK_SCHED_LEARNED) return fail(GK_ERR_ARG, "unknown scheduler mode");
+    if (force_accum < GK_ACCUM_AUTO || force_accum > GK_ACCUM_HASH) return fail(GK_ERR_ARG, "unknown accumulator");
+    if (sched == GK_SCHED_LEARNED && force_accum == GK_ACCUM_AUTO) GK_CHECK(ensure_model_on_device());
+    k_choose<<<1, NBINS, 0, s>>>(bins, var_of_bin, sched, force_accum, epi, values);
+    GK_CUDA(cudaGetLastError());
+    return GK_OK;
+}
+
+}  // namespace gk
+
+extern "C" {
+
+int gk_sched_num_variants(void) { return gk::NV; }
+int gk_sched_num_features(void) { return gk::NFEAT; }
+size_t gk_sched_model_size(void) { return static_cast<size_t>(gk::MLP_SIZE); }
+
+int gk_sched_set_model(const float *weights, size_t n_floats) {
+    if (!weights || n_floats != static_cast<size_t>(gk::MLP_SIZE))
+        return gk::fail(GK_ERR_ARG, "gk_sched_set_model: weight count does not match gk_sched_model_size()");
+    for (size_t i = 0; i < n_floats; ++i)
+        if (!std::isfinite(weights[i])) return gk::fail(GK_ERR_ARG, "gk_sched_set_model: non-finite weight");
+    std::lock_guard<std::mutex> lock(gk::g_model_mutex);
+    gk::g_model.assign(weights, weights + n_floats);
+    ++gk::g_model_version;
+    return GK_OK;
+}
+
+int gk_sched_has_model(void) {
+    std::lock_guard<std::mutex> lock(gk::g_model_mutex);
+    return gk::g_model.empty() ? 0 : 1;
+}
+
+}  // extern "C"

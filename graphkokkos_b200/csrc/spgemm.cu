@@ -1,0 +1,658 @@
+// Masked SpGEMM engine C<M> = A·B on sm_100a.
+//
+// Reference: mxmm_msa (include/matrix_la.h:562-635) and mxmm_mca (:478-528)
+// — a row-wise Gustavson product that, for every row i, streams the rows B_k
+// of the entries k of A_i and accumulates a·b at the columns that the mask
+// row M_i allows; C has exactly M's pattern.  The reference runs one row per
+// OpenMP thread with a dense accumulator of B.n entries per thread.
+//
+// B200 design (all device-side, no host synchronisation, graph-capturable):
+//  1. k_row_stats   one warp per row: work_i = sum_{k in A_i} nnz(B_k), max nnz(B_k)
+//  2. k_bin_rows    bin each row by (log2 nnz(M_i), log2 mean nnz(B_k)); per-bin stats
+//  3. sched_choose  one variant per bin (plain heuristic or learned MLP)
+//  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
+//                   get their item count (mask chunks x A-entry splits)
+//  5. one persistent kernel per variant over its rows / items:
+//       HASH_GROUP  G in {4,8,16,32} threads per row, the mask row's columns in a
+//                   shared-memory hash set (slot = accumulator)
+//       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
+//                   binary search (mask-compressed accumulator, matrix_la.h:437-461)
+//       HASH_BLOCK  one CTA per item, 8K/32K-slot hash set, warps take A entries
+//                   dynamically; heavy rows split over several CTAs
+//       MCA_BLOCK   one CTA per item, up to 16K sorted mask columns
+//       MSA_BLOCK   one CTA per item, dense column-window accumulator
+//                   (the reference's MSA, matrix_la.h:611-631) or bitmap
+// B rows are streamed with 16-byte vector loads; mask chunks that do not cover
+// a whole mask row only stream the part of B_k inside the chunk's column range
+// (group-cooperative search).  Integer terms are summed in 32-bit wrapping
+// arithmetic, so any assignment of rows to variants gives identical values.
+#include <cub/cub.cuh>
+
+#include "gk_common.cuh"
+#include "gk_device.cuh"
+#include "gk_sched.cuh"
+#include "gk_spgemm.cuh"
+
+namespace gk {
+
+// ---------------------------------------------------------------------------
+// kernel arguments
+// ---------------------------------------------------------------------------
+struct KArgs {
+    DevCsr A, B, M;
+    const int32_t *rowlist;  // rows sorted by variant
+    const int *voff;         // [NV+1] offsets into rowlist
+    const int64_t *item_ex;  // exclusive prefix of items per rowlist entry (block kinds)
+    const int64_t *work;     // per-row work
+    unsigned int *fetch;     // [NV] dynamic item counters (block kinds)
+    int32_t *c_val;
+    unsigned long long *sums;
+    const int32_t *row_key;
+    int v;    // variant id
+    int vec;  // B.col is 16-byte aligned: vector loads allowed
+};
+
+// ---------------------------------------------------------------------------
+// streaming helper: calls probe(x, b) for every element of B_k[b0, b1)
+// handled by this lane (lanes of a group of G stride the row).
+// ---------------------------------------------------------------------------
+template <int G, bool VAL, class F>
+__device__ __forceinline__ void stream_brow(const KArgs &p, int64_t b0, int64_t b1, int lane, F &&probe) {
+    const int32_t *__restrict__ bc = p.B.col;
+    if (!VAL && p.vec) {
+        int64_t h1 = (b0 + 3) & ~int64_t(3);
+        if (h1 > b1) h1 = b1;
+        if (b0 + lane < h1) probe(__ldg(bc + b0 + lane), 1u);
+        const int64_t v0 = h1 >> 2, v1 = b1 >> 2;
+        const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
+#pragma unroll 2
+        for (int64_t q = v0 + lane; q < v1; q += G) {
+            const int4 x = __ldg(bv + q);
+            probe(x.x, 1u);
+            probe(x.y, 1u);
+            probe(x.z, 1u);
+            probe(x.w, 1u);
+        }
+        int64_t tl = v1 << 2;
+        if (tl < h1) tl = h1;
+        if (tl + lane < b1) probe(__ldg(bc + tl + lane), 1u);
+    } else {
+        const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
+        for (int64_t j = b0 + lane; j < b1; j += G)
+            probe(__ldg(bc + j), (VAL && bvals) ? static_cast<uint32_t>(__ldg(bvals + j)) : 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// plan kernels
+// ---------------------------------------------------------------------------
+__global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < A.m; r += warps) {
+        const int64_t a0 = A.rp[r], a1 = A.rp[r + 1];
+        long long w = 0;
+        int mb = 0;
+        for (int64_t t = a0 + lane; t < a1; t += 32) {
+            const int k = __ldg(A.col + t);
+            const int len = static_cast<int>(__ldg(B.rp + k + 1) - __ldg(B.rp + k));
+            w += len;
+            mb = max(mb, len);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            w += __shfl_xor_sync(0xFFFFFFFFu, w, o);
+            mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+        }
+        if (lane == 0) {
+            work[r] = w;
+            maxb[r] = mb;
+        }
+    }
+}
+
+__global__ void k_bin_rows(DevCsr A, DevCsr M, const int64_t *work, const int32_t *maxb, uint16_t *bin,
+                           BinStats *bins) {
+    __shared__ unsigned long long s_rows[NBINS], s_m[NBINS], s_a[NBINS], s_w[NBINS];
+    __shared__ unsigned int s_b[NBINS];
+    for (int b = threadIdx.x; b < NBINS; b += blockDim.x) {
+        s_rows[b] = s_m[b] = s_a[b] = s_w[b] = 0;
+        s_b[b] = 0;
+    }
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.m; r += stride) {
+        const int64_t mlen = M.rp[r + 1] - M.rp[r];
+        const int64_t alen = A.rp[r + 1] - A.rp[r];
+        const int64_t w = work[r];
+        if (mlen == 0 || w == 0) {
+            bin[r] = BIN_SKIP;
+            continue;
+        }
+        const int qm = min(NB_M - 1, ilog2_u64(static_cast<unsigned long long>(mlen)));
+        const int qb = min(NB_B - 1, ilog2_u64(static_cast<unsigned long long>(w / alen)));
+        const int b = qm * NB_B + qb;
+        bin[r] = static_cast<uint16_t>(b);
+        atomicAdd(&s_rows[b], 1ull);
+        atomicAdd(&s_m[b], static_cast<unsigned long long>(mlen));
+        atomicAdd(&s_a[b], static_cast<unsigned long long>(alen));
+        atomicAdd(&s_w[b], static_cast<unsigned long long>(w));
+        atomicMax(&s_b[b], static_cast<unsigned int>(maxb[r]));
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < NBINS; b += blockDim.x) {
+        if (s_rows[b] == 0) continue;
+        atomicAdd(&bins[b].rows, s_rows[b]);
+        atomicAdd(&bins[b].sum_m, s_m[b]);
+        atomicAdd(&bins[b].sum_a, s_a[b]);
+        atomicAdd(&bins[b].sum_work, s_w[b]);
+        atomicMax(&bins[b].max_b, s_b[b]);
+    }
+}
+
+__device__ __forceinline__ int64_t items_of_row(int v, bool write, int64_t mlen, int64_t alen, int64_t w,
+                                                const int32_t *mcol_row) {
+    const Variant V = c_variants[v];
+    if (V.kind == K_HASH_GROUP || V.kind == K_MCA_GROUP) return 1;
+    int64_t nch;
+    if (V.kind == K_MSA_BLOCK) {
+        const int lw = write ? V.cap_write : V.cap;
+        nch = (int64_t)(mcol_row[mlen - 1] >> lw) - (int64_t)(mcol_row[0] >> lw) + 1;
+    } else {
+        const int ch = write ? V.chunk_write : V.chunk;
+        nch = (mlen + ch - 1) / ch;
+    }
+    return nch * num_splits(w, alen, V.split_log2);
+}
+
+// Counting sort of the rows by variant, one CTA-level reservation per variant.
+__global__ void k_count_rows(int64_t m, const uint16_t *bin, const int *var_of_bin, int force_variant,
+                             int *vcount) {
+    __shared__ int s_cnt[NV];
+    if (threadIdx.x < NV) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += stride) {
+        const uint16_t b = bin[r];
+        if (b == BIN_SKIP) continue;
+        const int v = force_variant >= 0 ? force_variant : var_of_bin[b];
+        atomicAdd(&s_cnt[v], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < NV && s_cnt[threadIdx.x]) atomicAdd(&vcount[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void k_offsets(const int *vcount, int *voff, int *vcursor, unsigned int *fetch) {
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int v = 0; v < NV; ++v) {
+            voff[v] = acc;
+            vcursor[v] = acc;
+            fetch[v] = 0;
+            acc += vcount[v];
+        }
+        voff[NV] = acc;
+    }
+}
+
+__global__ void k_scatter_rows(DevCsr A, DevCsr M, const int64_t *work, const uint16_t *bin,
+                               const int *var_of_bin, int force_variant, bool write, int *vcursor,
+                               int32_t *rowlist, int64_t *item_n) {
+    __shared__ int s_cnt[NV], s_base[NV];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < A.m; base += stride) {
+        if (threadIdx.x < NV) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const int64_t r = base + threadIdx.x;
+        int v = -1, local = 0;
+        if (r < A.m) {
+            const uint16_t b = bin[r];
+            if (b != BIN_SKIP) {
+                v = force_variant >= 0 ? force_variant : var_of_bin[b];
+                local = atomicAdd(&s_cnt[v], 1);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < NV && s_cnt[threadIdx.x]) s_base[threadIdx.x] = atomicAdd(&vcursor[threadIdx.x], s_cnt[threadIdx.x]);
+        __syncthreads();
+        if (v >= 0) {
+            const int pos = s_base[v] + local;
+            rowlist[pos] = static_cast<int32_t>(r);
+            const int64_t m0 = M.rp[r], mlen = M.rp[r + 1] - m0;
+            item_n[pos] = items_of_row(v, write, mlen, A.rp[r + 1] - A.rp[r], work[r], M.col + m0);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// group kinds: one row per group of G threads
+// ---------------------------------------------------------------------------
+template <int G, int NT, int CAP, int CHUNK, bool MCA, int EPI, bool VAL>
+__global__ void __launch_bounds__(NT) k_group(KArgs p) {
+    constexpr int NG = NT / G;
+    constexpr bool ACC = (EPI == EPI_WRITE);
+    extern __shared__ int smem[];
+    __shared__ unsigned long long s_red[NT / 32];
+    const int g = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    int *keys = smem + g * CAP;
+    int *acc = smem + NG * CAP + g * CAP;
+    const unsigned gmask = group_mask<G>();
+    const int begin = p.voff[p.v], end = p.voff[p.v + 1];
+    unsigned long long local = 0;
+
+    for (int idx = begin + blockIdx.x * NG + g; idx < end; idx += gridDim.x * NG) {
+        const int row = p.rowlist[idx];
+        const int64_t m0 = p.M.rp[row];
+        const int mlen = static_cast<int>(p.M.rp[row + 1] - m0);
+        const int64_t a0 = p.A.rp[row], a1 = p.A.rp[row + 1];
+        const int32_t *__restrict__ mc = p.M.col + m0;
+        const bool chunked = mlen > CHUNK;
+        unsigned long long rowsum = 0;
+        for (int c0 = 0; c0 < mlen; c0 += CHUNK) {
+            const int c1 = min(mlen, c0 + CHUNK);
+            const int clen = c1 - c0;
+            if (MCA) {
+                for (int q = lane; q < clen; q += G) {
+                    keys[q] = mc[c0 + q];
+                    if (ACC) acc[q] = 0;
+                }
+            } else {
+                for (int s = lane; s < CAP; s += G) {
+                    keys[s] = EMPTY_KEY;
+                    if (ACC) acc[s] = 0;
+                }
+                __syncwarp(gmask);
+                for (int q = c0 + lane; q < c1; q += G) hash_insert<CAP>(keys, mc[q]);
+            }
+            __syncwarp(gmask);
+            const int lo_col = mc[c0], hi_col = mc[c1 - 1];
+            unsigned cnt = 0;
+            for (int64_t t = a0; t < a1; ++t) {
+                const int k = __ldg(p.A.col + t);
+                const uint32_t av = (VAL && p.A.val) ? static_cast<uint32_t>(__ldg(p.A.val + t)) : 1u;
+                int64_t b0 = __ldg(p.B.rp + k), b1 = __ldg(p.B.rp + k + 1);
+                if (b0 >= b1) continue;
+                if (chunked) {
+                    if (__ldg(p.B.col + b1 - 1) < lo_col || __ldg(p.B.col + b0) > hi_col) continue;
+                    b0 = group_lower_bound<G>(p.B.col, b0, b1, lo_col, lane, gmask);
+                    b1 = group_lower_bound<G>(p.B.col, b0, b1, hi_col + 1, lane, gmask);
+                }
+                stream_brow<G, VAL>(p, b0, b1, lane, [&](int x, uint32_t bv) {
+                    const int s = MCA ? sorted_find(keys, clen, x) : hash_find<CAP>(keys, x);
+                    if (s >= 0) {
+                        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), av * bv);
+                        else cnt += av * bv;
+                    }
+                });
+            }
+            if (ACC) {
+                __syncwarp(gmask);
+                for (int q = c0 + lane; q < c1; q += G) {
+                    const int s = MCA ? (q - c0) : hash_find<CAP>(keys, mc[q]);
+                    p.c_val[m0 + q] = acc[s];
+                }
+            } else {
+                rowsum += cnt;
+            }
+            __syncwarp(gmask);
+        }
+        if (EPI == EPI_SUM) local += rowsum;
+        if (EPI == EPI_KEYED) {
+            const unsigned long long tot = group_sum<G>(rowsum, gmask);
+            if (lane == 0 && tot) atomicAdd(p.sums + (p.row_key ? p.row_key[row] : row), tot);
+        }
+    }
+    if (EPI == EPI_SUM) {
+        const unsigned long long tot = block_sum(local, s_red);
+        if (threadIdx.x == 0 && tot) atomicAdd(p.sums, tot);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// block kinds: one item (row, mask chunk or column window, A-entry split) per CTA
+// ---------------------------------------------------------------------------
+template <int NT, int KIND, int CAP, int CHUNK, int SPLIT, int EPI, bool VAL>
+__global__ void __launch_bounds__(NT) k_block(KArgs p) {
+    constexpr bool ACC = (EPI == EPI_WRITE);
+    constexpr int NW = NT / 32;
+    // MSA: CAP is log2 of the window width in columns
+    constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;
+    extern __shared__ int smem[];
+    __shared__ unsigned long long s_red[NW];
+    __shared__ int64_t s_item;
+    __shared__ int s_pos;
+    __shared__ int s_next;
+    const int lane = threadIdx.x & 31;
+    const int begin = p.voff[p.v], end = p.voff[p.v + 1];
+    if (begin == end) return;
+    const int64_t ibeg = p.item_ex[begin], iend = p.item_ex[end];
+    unsigned long long local = 0;
+
+    while (true) {
+        if (threadIdx.x == 0) {
+            const int64_t I = ibeg + static_cast<int64_t>(atomicAdd(p.fetch + p.v, 1u));
+            s_item = I;
+            if (I < iend) {  // last rowlist position whose prefix <= I
+                int lo = begin, hi = end;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (p.item_ex[mid] <= I) lo = mid;
+                    else hi = mid;
+                }
+                s_pos = lo;
+            }
+        }
+        __syncthreads();
+        const int64_t I = s_item;
+        if (I >= iend) break;
+        const int pos = s_pos;
+        const int row = p.rowlist[pos];
+        const int64_t l = I - p.item_ex[pos];
+        const int64_t m0 = p.M.rp[row];
+        const int mlen = static_cast<int>(p.M.rp[row + 1] - m0);
+        const int64_t a0 = p.A.rp[row], alen = p.A.rp[row + 1] - a0;
+        const int64_t nsp = num_splits(p.work[row], alen, SPLIT);
+        const int64_t ch = l / nsp, sp = l % nsp;
+        const int64_t t0 = a0 + alen * sp / nsp, t1 = a0 + alen * (sp + 1) / nsp;
+        const int32_t *__restrict__ mc = p.M.col + m0;
+
+        // ---- build the mask structure of this item ----
+        int c0, c1;       // mask positions covered
+        int lo_col, hi_col;
+        int *keys = smem;
+        int *acc = smem + ((KIND == K_MSA_BLOCK) ? (ACC ? WIN / 32 : 0) : CAP);
+        unsigned *bits = reinterpret_cast<unsigned *>(smem);
+        bool cut;
+        if constexpr (KIND == K_MSA_BLOCK) {
+            const int64_t wbase = ((int64_t)(mc[0] >> CAP) + ch) << CAP;
+            lo_col = static_cast<int>(wbase);
+            { const int64_t hc = wbase + WIN - 1; hi_col = static_cast<int>(hc < 0x7FFFFFFF ? hc : 0x7FFFFFFF); }
+            // mask positions inside the window
+            int lo = 0, hi = mlen;
+            while (lo < hi) { const int md = (lo + hi) >> 1; if (mc[md] < lo_col) lo = md + 1; else hi = md; }
+            c0 = lo;
+            hi = mlen;
+            while (lo < hi) { const int md = (lo + hi) >> 1; if (mc[md] <= hi_col) lo = md + 1; else hi = md; }
+            c1 = lo;
+            for (int wd = threadIdx.x; wd < WIN / 32; wd += NT) bits[wd] = 0u;
+            __syncthreads();
+            for (int q = c0 + threadIdx.x; q < c1; q += NT) {
+                const int x = mc[q] - lo_col;
+                atomicOr(bits + (x >> 5), 1u << (x & 31));
+                if (ACC) acc[x] = 0;
+            }
+            cut = (mc[0] >> CAP) != (mc[mlen - 1] >> CAP);
+        } else {
+            const int CH = CHUNK;
+            c0 = static_cast<int>(ch) * CH;
+            c1 = min(mlen, c0 + CH);
+            if constexpr (KIND == K_MCA_BLOCK) {
+                for (int q = threadIdx.x; q < c1 - c0; q += NT) {
+                    keys[q] = mc[c0 + q];
+                    if (ACC) acc[q] = 0;
+                }
+            } else {
+                for (int s = threadIdx.x; s < CAP; s += NT) {
+                    keys[s] = EMPTY_KEY;
+                    if (ACC) acc[s] = 0;
+                }
+                __syncthreads();
+                for (int q = c0 + threadIdx.x; q < c1; q += NT) hash_insert<CAP>(keys, mc[q]);
+            }
+            lo_col = mc[c0];
+            hi_col = mc[c1 - 1];
+            cut = mlen > CH;
+        }
+        if (threadIdx.x == 0) s_next = static_cast<int>(0);
+        __syncthreads();
+
+        // ---- stream the B rows of A entries [t0, t1), one entry per warp at a time ----
+        unsigned cnt = 0;
+        const int clen = c1 - c0;
+        if (c1 > c0) {
+            while (true) {
+                int tt = 0;
+                if (lane == 0) tt = atomicAdd(&s_next, 1);
+                tt = __shfl_sync(0xFFFFFFFFu, tt, 0);
+                const int64_t t = t0 + tt;
+                if (t >= t1) break;
+                const int k = __ldg(p.A.col + t);
+                const uint32_t av = (VAL && p.A.val) ? static_cast<uint32_t>(__ldg(p.A.val + t)) : 1u;
+                int64_t b0 = __ldg(p.B.rp + k), b1 = __ldg(p.B.rp + k + 1);
+                if (b0 >= b1) continue;
+                if (__ldg(p.B.col + b1 - 1) < lo_col || __ldg(p.B.col + b0) > hi_col) continue;
+                if (cut) {
+                    b0 = group_lower_bound<32>(p.B.col, b0, b1, lo_col, lane, 0xFFFFFFFFu);
+                    b1 = group_lower_bound<32>(p.B.col, b0, b1, hi_col + 1, lane, 0xFFFFFFFFu);
+                }
+                stream_brow<32, VAL>(p, b0, b1, lane, [&](int x, uint32_t bv) {
+                    int s;
+                    if constexpr (KIND == K_MSA_BLOCK) {
+                        const int y = x - lo_col;
+                        s = (y >= 0 && y < WIN && ((bits[y >> 5] >> (y & 31)) & 1u)) ? y : -1;
+                    } else if constexpr (KIND == K_MCA_BLOCK) {
+                        s = sorted_find(keys, clen, x);
+                    } else {
+                        s = hash_find<CAP>(keys, x);
+                    }
+                    if (s >= 0) {
+                        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), av * bv);
+                        else cnt += av * bv;
+                    }
+                });
+            }
+        }
+        __syncthreads();
+
+        // ---- epilogue ----
+        if (ACC) {
+            for (int q = c0 + threadIdx.x; q < c1; q += NT) {
+                int s;
+                if constexpr (KIND == K_MSA_BLOCK) s = mc[q] - lo_col;
+                else if constexpr (KIND == K_MCA_BLOCK) s = q - c0;
+                else s = hash_find<CAP>(keys, mc[q]);
+                const int val = acc[s];
+                if (nsp == 1) p.c_val[m0 + q] = val;
+                else if (val) atomicAdd(p.c_val + m0 + q, val);
+            }
+        } else if (EPI == EPI_KEYED) {
+            const unsigned long long tot = block_sum(static_cast<unsigned long long>(cnt), s_red);
+            if (threadIdx.x == 0 && tot) atomicAdd(p.sums + (p.row_key ? p.row_key[row] : row), tot);
+        } else {
+            local += cnt;
+        }
+        __syncthreads();
+    }
+    if (EPI == EPI_SUM) {
+        const unsigned long long tot = block_sum(local, s_red);
+        if (threadIdx.x == 0 && tot) atomicAdd(p.sums, tot);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side: launching one variant
+// ---------------------------------------------------------------------------
+template <int V>
+constexpr size_t smem_bytes(bool write) {
+    constexpr Variant X = VARIANTS[V];
+    if constexpr (X.kind == K_HASH_GROUP || X.kind == K_MCA_GROUP) {
+        const int nt = group_cta_threads(V);
+        const int ng = nt / X.G;
+        const int cap = (X.kind == K_MCA_GROUP) ? X.chunk : X.cap;
+        return size_t(ng) * cap * 4 * (write ? 2 : 1);
+    } else if constexpr (X.kind == K_MSA_BLOCK) {
+        if (write) return (size_t(1) << X.cap_write) / 8 + (size_t(1) << X.cap_write) * 4;
+        return (size_t(1) << X.cap) / 8;
+    } else {
+        const int cap = write ? X.cap_write : X.cap;
+        return size_t(cap) * 4 * (write ? 2 : 1);
+    }
+}
+
+template <int V, int EPI, bool VAL>
+static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t s) {
+    constexpr Variant X = VARIANTS[V];
+    constexpr bool W = (EPI == EPI_WRITE);
+    constexpr size_t SMEM = smem_bytes<V>(W);
+    void (*fn)(KArgs);
+    int nt;
+    if constexpr (X.kind == K_HASH_GROUP || X.kind == K_MCA_GROUP) {
+        constexpr int NTV = (V == 4) ? 128 : NT_GROUP;
+        constexpr bool MCA = X.kind == K_MCA_GROUP;
+        constexpr int CAPV = MCA ? X.chunk : X.cap;
+        fn = k_group<X.G, NTV, CAPV, X.chunk, MCA, EPI, VAL>;
+        nt = NTV;
+    } else {
+        constexpr int CAPV = (X.kind == K_MSA_BLOCK) ? (W ? X.cap_write : X.cap) : (W ? X.cap_write : X.cap);
+        constexpr int CHV = W ? X.chunk_write : X.chunk;
+        fn = k_block<X.G, X.kind, CAPV, CHV, X.split_log2, EPI, VAL>;
+        nt = X.G;
+    }
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SMEM));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, SMEM);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    fn<<<num_sms * per_sm, nt, SMEM, s>>>(args);
+    return cudaGetLastError();
+}
+
+template <int V>
+static cudaError_t launch_variant_v(const KArgs &a, int epi, bool val, int sms, cudaStream_t s) {
+    if (epi == EPI_WRITE) return val ? launch_variant_t<V, EPI_WRITE, true>(a, sms, s)
+                                     : launch_variant_t<V, EPI_WRITE, false>(a, sms, s);
+    if (epi == EPI_SUM) return launch_variant_t<V, EPI_SUM, false>(a, sms, s);
+    return launch_variant_t<V, EPI_KEYED, false>(a, sms, s);
+}
+
+static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int sms, cudaStream_t s) {
+    switch (v) {
+        case 0: return launch_variant_v<0>(a, epi, val, sms, s);
+        case 1: return launch_variant_v<1>(a, epi, val, sms, s);
+        case 2: return launch_variant_v<2>(a, epi, val, sms, s);
+        case 3: return launch_variant_v<3>(a, epi, val, sms, s);
+        case 4: return launch_variant_v<4>(a, epi, val, sms, s);
+        case 5: return launch_variant_v<5>(a, epi, val, sms, s);
+        case 6: return launch_variant_v<6>(a, epi, val, sms, s);
+        case 7: return launch_variant_v<7>(a, epi, val, sms, s);
+        case 8: return launch_variant_v<8>(a, epi, val, sms, s);
+        case 9: return launch_variant_v<9>(a, epi, val, sms, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
+    const DevCsr &A = rq.A, &B = rq.B, &M = rq.M;
+    if (A.m != M.m || A.n != B.m || B.n != M.n)
+        return fail(GK_ERR_ARG, "shape mismatch: need A.m == M.m, A.n == B.m, B.n == M.n");
+    cudaStream_t s = rq.stream;
+    Context &c = ctx();
+    const bool write = rq.epi == EPI_WRITE;
+    if (write && M.nnz > 0 && rq.zero_output) GK_CUDA(cudaMemsetAsync(rq.c_val, 0, sizeof(int32_t) * M.nnz, s));
+    if (A.m == 0 || M.nnz == 0 || A.nnz == 0 || B.nnz == 0) return GK_OK;
+
+    const int64_t m = A.m;
+    int64_t *work, *item_n, *item_ex;
+    int32_t *maxb, *rowlist;
+    uint16_t *bin;
+    BinStats *bins;
+    int *var_of_bin, *vcount, *voff, *vcursor;
+    unsigned int *fetch;
+    GK_CHECK(scr.alloc(&work, m));
+    GK_CHECK(scr.alloc(&maxb, m));
+    GK_CHECK(scr.alloc(&bin, m));
+    GK_CHECK(scr.alloc(&rowlist, m));
+    GK_CHECK(scr.alloc(&item_n, m + 1));
+    GK_CHECK(scr.alloc(&item_ex, m + 1));
+    GK_CHECK(scr.alloc(&bins, NBINS));
+    GK_CHECK(scr.alloc(&var_of_bin, NBINS));
+    GK_CHECK(scr.alloc(&vcount, 4 * NV + 4));
+    voff = vcount + NV;
+    vcursor = voff + NV + 1;
+    GK_CHECK(scr.alloc(&fetch, NV));
+    GK_CUDA(cudaMemsetAsync(bins, 0, sizeof(BinStats) * NBINS, s));
+    GK_CUDA(cudaMemsetAsync(vcount, 0, sizeof(int) * (4 * NV + 4), s));
+    GK_CUDA(cudaMemsetAsync(item_n, 0, sizeof(int64_t) * (m + 1), s));
+
+    const int sms = c.num_sms;
+    k_row_stats<<<sms * 8, 256, 0, s>>>(A, B, work, maxb);
+    GK_CUDA(cudaGetLastError());
+    k_bin_rows<<<sms * 2, 256, 0, s>>>(A, M, work, maxb, bin, bins);
+    GK_CUDA(cudaGetLastError());
+    if (rq.bin_variant) {
+        GK_CUDA(cudaMemcpyAsync(var_of_bin, rq.bin_variant, sizeof(int) * NBINS, cudaMemcpyHostToDevice, s));
+    } else if (rq.force_variant < 0) {
+        GK_CHECK(sched_choose(bins, var_of_bin, rq.sched, rq.force_accum, rq.epi, rq.use_values, s));
+    }
+    if (rq.bin_stats_out)
+        GK_CUDA(cudaMemcpyAsync(rq.bin_stats_out, bins, sizeof(BinStats) * NBINS, cudaMemcpyDeviceToDevice, s));
+    if (rq.variant_of_bin_out && rq.force_variant < 0)
+        GK_CUDA(cudaMemcpyAsync(rq.variant_of_bin_out, var_of_bin, sizeof(int) * NBINS, cudaMemcpyDeviceToDevice, s));
+    k_count_rows<<<sms * 2, 256, 0, s>>>(m, bin, var_of_bin, rq.force_variant, vcount);
+    GK_CUDA(cudaGetLastError());
+    k_offsets<<<1, 32, 0, s>>>(vcount, voff, vcursor, fetch);
+    GK_CUDA(cudaGetLastError());
+    k_scatter_rows<<<sms * 2, 256, 0, s>>>(A, M, work, bin, var_of_bin, rq.force_variant, write, vcursor,
+                                           rowlist, item_n);
+    GK_CUDA(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, item_n, item_ex, m + 1, s));
+    void *tmp;
+    GK_CHECK(scr.alloc(reinterpret_cast<char **>(&tmp), tmp_bytes));
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, item_n, item_ex, m + 1, s));
+
+    note_launches(5);
+
+    KArgs args;
+    args.A = A;
+    args.B = B;
+    args.M = M;
+    args.rowlist = rowlist;
+    args.voff = voff;
+    args.item_ex = item_ex;
+    args.work = work;
+    args.fetch = fetch;
+    args.c_val = rq.c_val;
+    args.sums = rq.sums;
+    args.row_key = rq.row_key;
+    args.vec = (reinterpret_cast<uintptr_t>(B.col) % 16) == 0;
+    const bool val = rq.use_values && (A.val || B.val);
+    ProfWindow prof(s, NV);
+    for (int v = 0; v < NV; ++v) {
+        if (rq.force_variant >= 0 && v != rq.force_variant) continue;
+        args.v = v;
+        prof.begin(v);
+        cudaError_t e = launch_variant(v, args, rq.epi, val, sms, s);
+        if (e != cudaSuccess) return cuda_fail(e, "masked SpGEMM variant launch");
+        prof.end(v);
+        note_launches(1);
+    }
+    if (prof.active()) {
+        // attribute the bins' work to the variants that ran them
+        BinStats hb[NBINS];
+        int hv[NBINS];
+        GK_CUDA(cudaMemcpyAsync(hb, bins, sizeof(hb), cudaMemcpyDeviceToHost, s));
+        GK_CUDA(cudaMemcpyAsync(hv, var_of_bin, sizeof(hv), cudaMemcpyDeviceToHost, s));
+        GK_CUDA(cudaStreamSynchronize(s));
+        ProfTotals tot[NV] = {};
+        for (int b = 0; b < NBINS; ++b) {
+            if (!hb[b].rows) continue;
+            const int v = rq.force_variant >= 0 ? rq.force_variant : (rq.bin_variant ? rq.bin_variant[b] : hv[b]);
+            if (v < 0 || v >= NV) continue;
+            tot[v].rows += hb[b].rows;
+            tot[v].sum_a += hb[b].sum_a;
+            tot[v].sum_m += hb[b].sum_m;
+            tot[v].sum_work += hb[b].sum_work;
+        }
+        GK_CHECK(prof.finish(tot));
+    }
+    return GK_OK;
+}
+
+}  // namespace gk

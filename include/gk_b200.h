@@ -1,0 +1,212 @@
+/*
+ * gk_b200.h — C ABI of the B200-native masked SpGEMM library.
+ *
+ * Drop-in boundary for GraphKokkos' hot path: the masked sparse
+ * matrix-matrix multiply C<M> = A·B and the algorithms built on it
+ * (triangle counting, k-truss, batched betweenness centrality).  The
+ * reference exposes these as C++ templates over host-resident Kokkos Views;
+ * this header exposes the same operations with plain pointers and sizes so
+ * that any host language can bind them.
+ *
+ * Conventions
+ *  - Matrices are CSR: int64 row pointers (m+1), int32 column indices sorted
+ *    ascending within each row, optional int32 values (NULL: every stored
+ *    value is 1, the adjacency convention of the reference's
+ *    build_adjacency_matrix, include/matrix.h:643-660).
+ *  - Every array pointer may be host memory or device memory of the current
+ *    CUDA device.  Host inputs are copied to HBM inside the call; host outputs
+ *    are copied back and the call returns after they are written.  With device
+ *    outputs the call is asynchronous on `stream` (a cudaStream_t; NULL = the
+ *    legacy default stream).
+ *  - Every entry point returns a gk_status; on failure gk_last_error_string()
+ *    describes the error for the calling host thread.  Calls on different
+ *    streams may run concurrently.
+ *  - Results are bit-exact with the reference on the same inputs: integer
+ *    outputs exactly, FP64 betweenness scores to round-off (the scheduler
+ *    changes only the order of FP64 sums).
+ */
+#ifndef GK_B200_H
+#define GK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports errors by throwing (include/matrix.h:45-60,
+ * include/matrix_la.h:291-292); the ABI returns codes instead. */
+typedef enum gk_status {
+    GK_OK = 0,
+    GK_ERR_ARG = 1,         /* bad argument (null pointer, shape mismatch, k < 3, ...) */
+    GK_ERR_OOM = 2,         /* device memory exhausted */
+    GK_ERR_CUDA = 3,        /* CUDA runtime error */
+    GK_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    GK_ERR_INVALID_CSR = 5, /* rowptr not monotone, column out of range or unsorted */
+    GK_ERR_UNSUPPORTED = 6  /* request outside what the library implements */
+} gk_status;
+
+/* Read-only CSR matrix (spMtx<T>, include/matrix.h:33-43: m, n, nz, Rst, Col, Val). */
+typedef struct gk_csr {
+    int64_t m, n, nnz;
+    const int64_t *rowptr; /* m+1 entries */
+    const int32_t *col;    /* nnz entries, sorted within each row */
+    const int32_t *val;    /* nnz entries, or NULL for "all ones" */
+} gk_csr;
+
+/* Mutable pattern-only CSR, used in place by gk_ktruss. */
+typedef struct gk_csr_mut {
+    int64_t m, n, nnz;
+    int64_t *rowptr; /* m+1 entries */
+    int32_t *col;    /* capacity >= nnz on entry */
+} gk_csr_mut;
+
+/* Semiring of the product.  PLUS_TIMES is the reference's arithmetic
+ * (accum(j) += a·b, include/matrix_la.h:624); PLUS_PAIR treats every stored
+ * value as 1 (what triangle counting and k-truss compute on adjacency
+ * matrices, whose values are all 1). */
+typedef enum gk_semiring { GK_PLUS_TIMES = 0, GK_PLUS_PAIR = 1 } gk_semiring;
+
+/* Row-bin scheduler.  PLAIN: the hand-written binning heuristic.  LEARNED:
+ * the MLP loaded with gk_sched_set_model (GK_ERR_ARG if none is loaded).
+ * The scheduler changes only which kernel variant processes a row, never the
+ * arithmetic. */
+typedef enum gk_sched { GK_SCHED_PLAIN = 0, GK_SCHED_LEARNED = 1 } gk_sched;
+
+/* Accumulator families a caller may force (GK_ACCUM_AUTO lets the scheduler
+ * choose).  MSA and MCA name the reference's two live accumulators
+ * (include/matrix_la.h:562-694 and :478-528). */
+typedef enum gk_accum {
+    GK_ACCUM_AUTO = 0,
+    GK_ACCUM_MSA = 1,  /* dense column-window accumulator in shared memory */
+    GK_ACCUM_MCA = 2,  /* mask-compressed: slots = mask positions, binary search */
+    GK_ACCUM_HASH = 3  /* hash of mask columns in shared memory */
+} gk_accum;
+
+/* C<M> = A·B.  Replaces the reference operator type
+ *   mxmOp<T> = void(*)(bool, const spMtx<T>& A, const spMtx<T>& B,
+ *                      const spMtx<T>& M, spMtx<T>& C)      (src/main.cpp:13-14)
+ * implemented by mxmm_msa (include/matrix_la.h:562-635), mxmm_mca (:478-528)
+ * and mxmm_naive (:936-1068).  C has exactly M's pattern, explicit zeros kept
+ * (include/matrix_la.h:564-568): the ABI writes the nnz(M) values only,
+ * parallel to M's col array, into C_val.  Requires A.m == M.m, A.n == B.m,
+ * B.n == M.n.  `accum` forces an accumulator family (GK_ACCUM_AUTO: the
+ * scheduler picks per row bin). */
+int gk_mxmm_masked(const gk_csr *A, const gk_csr *B, const gk_csr *M, int32_t *C_val,
+                   int semiring, int sched, int accum, void *stream);
+
+/* Triangle count of the graph whose strict lower triangle is L:
+ * sum of C<L> = L·L (plus-pair), as triangle_counting_masked_sandia
+ * (src/main.cpp:69-90, after its untimed extract_lower_triangle at :71).
+ * *count receives the uint64 total (the reference returns int64). */
+int gk_tc_count(const gk_csr *L, uint64_t *count, int sched, void *stream);
+
+/* Per-vertex sums of C<L> = L·L: row_sums[i] = sum_j C(i,j), the number of
+ * triangles whose largest vertex is i (a fused-epilogue variant of
+ * triangle_counting_vertex, src/main.cpp:16-39). */
+int gk_tc_row_sums(const gk_csr *L, uint64_t *row_sums, int sched, void *stream);
+
+/* Triangle counts of many independent graphs in one persistent launch:
+ * counts[g] = gk_tc_count(&graphs[g]).  No reference counterpart (the
+ * reference runs one graph per process, src/main.cpp:323-345). */
+int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int sched, void *stream);
+
+/* k-truss of a symmetric adjacency matrix, in place: repeat S<C> = C·C,
+ * keep the entries with S >= k-2, until nnz stops changing (k_truss,
+ * src/main.cpp:94-141, with its View-size defect at :99/:118 not
+ * reproduced).  On return inout->rowptr/col/nnz hold the truss and *iters the
+ * number of passes (the reference's "Iterations:" line, :138).  k >= 3. */
+int gk_ktruss(gk_csr_mut *inout, int k, int *iters, int sched, void *stream);
+
+/* Batched betweenness centrality in FP64 over the given sources:
+ * bc[v] = sum over sources s of Brandes' dependency delta_s(v), unnormalised,
+ * as betweenness_centrality_batch (include/betweenness_centrality.h:406-506)
+ * computes for sources 0..b-1 (:445-447).  A must be square.  bc has A.m
+ * entries.  Sources must be distinct vertices. */
+int gk_bc_batch(const gk_csr *A, const int32_t *sources, int nsources, double *bc, int sched,
+                void *stream);
+
+/* Same operations with every row forced onto one kernel variant
+ * (0 <= variant < gk_sched_num_variants()): used to check each variant on its
+ * own and by the autotuner.  No reference counterpart. */
+int gk_tc_count_variant(const gk_csr *L, int variant, uint64_t *count, void *stream);
+int gk_mxmm_masked_variant(const gk_csr *A, const gk_csr *B, const gk_csr *M, int32_t *C_val, int semiring,
+                           int variant, void *stream);
+
+/* ----- CSR transforms (device or host arrays; outputs sized by the caller) ----- */
+
+/* Strict lower triangle (extract_lower_triangle, include/matrix.h:698-726).
+ * out_rowptr: m+1; out_col capacity >= nnz(A) (the result has *out_nnz). */
+int gk_extract_lower(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int64_t *out_nnz,
+                     void *stream);
+
+/* CSR transpose (transpose, include/matrix_la.h:155-179).  out_rowptr: n+1,
+ * out_col/out_val: nnz (out_val may be NULL). */
+int gk_transpose(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
+                 void *stream);
+
+/* ----- graph generation (device-side builder; host twin: gk_gen_*_host) ------- */
+
+/* Seeded RMAT graph (2^scale vertices, edge_factor << scale edges) or
+ * Erdos-Renyi G(n, nedges), symmetrised, self-loops and duplicates removed,
+ * rows sorted.  Two calls: first with rowptr == NULL to learn *nnz (m is known
+ * to the caller), then with device or host arrays of m+1 and nnz entries. */
+int gk_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                int64_t *nnz, int64_t *rowptr, int32_t *col, void *stream);
+int gk_gen_er(int64_t n, int64_t nedges, uint64_t seed, int64_t *nnz, int64_t *rowptr, int32_t *col,
+              void *stream);
+
+/* Host builders producing the identical CSR (C++/OpenMP). */
+typedef struct gk_host_graph gk_host_graph;
+int gk_gen_rmat_host(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                     gk_host_graph **out);
+int gk_gen_er_host(int64_t n, int64_t nedges, uint64_t seed, gk_host_graph **out);
+int gk_host_graph_info(const gk_host_graph *g, int64_t *m, int64_t *nnz);
+int gk_host_graph_copy(const gk_host_graph *g, int64_t *rowptr, int32_t *col);
+void gk_host_graph_free(gk_host_graph *g);
+
+/* ----- scheduler ------------------------------------------------------------ */
+
+/* Number of kernel variants the scheduler chooses among, and of the per-bin
+ * features the learned model reads. */
+int gk_sched_num_variants(void);
+int gk_sched_num_features(void);
+
+/* Loads the learned scheduler's MLP (float32 weights, layout documented in
+ * graphkokkos_b200/sched.py); n_floats must match gk_sched_model_size(). */
+size_t gk_sched_model_size(void);
+int gk_sched_set_model(const float *weights, size_t n_floats);
+int gk_sched_has_model(void);
+
+/* ----- profiling (no reference counterpart; the reference prints chrono
+ * brackets, src/main.cpp:74-86) -------------------------------------------------- */
+
+/* One record per kernel-variant launch of a masked SpGEMM call made while
+ * profiling is on: CUDA-event time of the launch and the rows / A entries /
+ * mask entries / streamed B entries (work) it processed.
+ * Mode 1 synchronises the stream after each call and fills the work fields;
+ * mode 2 only brackets the launches with events (no synchronisation, work
+ * fields 0) and gk_prof_flush() resolves them; mode 0 turns profiling off. */
+typedef struct gk_prof_rec {
+    int variant;
+    float ms;
+    int64_t rows, sum_a, sum_m, sum_work;
+} gk_prof_rec;
+int gk_prof_enable(int mode); /* also clears the records */
+int gk_prof_flush(void);
+int gk_prof_count(void);
+int gk_prof_get(int i, gk_prof_rec *out);
+
+/* Number of the library's own kernels launched so far in this process. */
+int64_t gk_launch_count(void);
+
+/* ----- misc ------------------------------------------------------------------- */
+const char *gk_last_error_string(void);
+int gk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GK_B200_H */

@@ -1,0 +1,292 @@
+"""Oracle bindings — TEST INFRASTRUCTURE ONLY.
+
+Loads the CPU restatement (oracle/_build/libgk_oracle.so, built from
+oracle/gk_oracle.cpp) and, when it was built, the reference compiled against
+the Kokkos-API shim (oracle/_ref/libgk_ref.so).  Only tests/, the smoke check
+and bench.py's CPU-baseline leg may import this package; the product never
+does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_PATH = os.path.join(HERE, "_build", "libgk_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libgk_ref.so")
+
+_port = None
+_ref = None
+
+
+def build(ref=True):
+    """Builds the port (always) and the reference oracle (when the reference
+    sources are present)."""
+    targets = ["port", "ref"] if ref else ["port"]
+    out = subprocess.run(["make", "-C", HERE] + targets, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{out.stdout}\n{out.stderr}")
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_PATH):
+            build(ref=False)
+        _port = ctypes.CDLL(PORT_PATH)
+    return _port
+
+
+def ref_available():
+    return os.path.exists(REF_PATH)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_PATH):
+            raise RuntimeError("reference oracle oracle/_ref/libgk_ref.so was not built")
+        _ref = ctypes.CDLL(REF_PATH)
+    return _ref
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _host(csr):
+    """(m, n, rowptr int64, col int32, val int32|None) as contiguous numpy."""
+    rp = np.ascontiguousarray(np.asarray(csr.rowptr if not hasattr(csr.rowptr, "cpu") else csr.rowptr.cpu().numpy(),
+                                         dtype=np.int64))
+    col = np.ascontiguousarray(np.asarray(csr.col if not hasattr(csr.col, "cpu") else csr.col.cpu().numpy(),
+                                          dtype=np.int32))
+    val = None
+    if csr.val is not None:
+        v = csr.val.cpu().numpy() if hasattr(csr.val, "cpu") else csr.val
+        val = np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+    return csr.m, csr.n, rp, col[: int(rp[-1])], val
+
+
+I64 = ctypes.c_int64
+
+
+# ----- port (restatement) -------------------------------------------------------
+def tc_lower(L):
+    m, _, rp, col, _ = _host(L)
+    out = ctypes.c_uint64(0)
+    port().orc_tc_lower(I64(m), _p(rp), _p(col), ctypes.byref(out))
+    return int(out.value)
+
+
+def tc_rows(L, row_begin, row_end):
+    m, _, rp, col, _ = _host(L)
+    out = ctypes.c_uint64(0)
+    port().orc_tc_rows(I64(m), _p(rp), _p(col), I64(row_begin), I64(row_end), ctypes.byref(out))
+    return int(out.value)
+
+
+def tc_row_stride(L, stride, offset=0, kind="reference"):
+    """Bounded CPU sample of triangle counting: rows i % stride == offset.
+    kind "reference": the reference's mxmm_msa (oracle/_ref); "port": the
+    restatement.  Returns (partial count, sampled nnz, seconds, threads)."""
+    m, _, rp, col, _ = _host(L)
+    out = ctypes.c_int64(0) if kind == "reference" else ctypes.c_uint64(0)
+    nz = ctypes.c_int64(0)
+    sec = ctypes.c_double(0.0)
+    lib = ref() if kind == "reference" else port()
+    fn = lib.ref_tc_row_stride if kind == "reference" else lib.orc_tc_row_stride
+    r = fn(I64(m), _p(rp), _p(col), I64(stride), I64(offset), ctypes.byref(out), ctypes.byref(nz), ctypes.byref(sec))
+    if r != 0:
+        raise RuntimeError("tc_row_stride failed")
+    threads = ref().ref_get_threads() if kind == "reference" else os.cpu_count()
+    return int(out.value), int(nz.value), float(sec.value), int(threads)
+
+
+def tc_merge(L):
+    m, _, rp, col, _ = _host(L)
+    out = ctypes.c_uint64(0)
+    port().orc_tc_merge(I64(m), _p(rp), _p(col), ctypes.byref(out))
+    return int(out.value)
+
+
+def tc_row_sums(L):
+    m, _, rp, col, _ = _host(L)
+    out = np.zeros(m, dtype=np.uint64)
+    port().orc_tc_row_sums(I64(m), _p(rp), _p(col), _p(out))
+    return out
+
+
+def mxmm(A, B, M):
+    am, an, arp, acol, aval = _host(A)
+    bm, bn, brp, bcol, bval = _host(B)
+    mm, mn, mrp, mcol, _ = _host(M)
+    out = np.zeros(int(mrp[-1]), dtype=np.int32)
+    r = port().orc_mxmm_masked(I64(am), I64(an), _p(arp), _p(acol), _p(aval), I64(bm), I64(bn), _p(brp), _p(bcol),
+                               _p(bval), I64(mm), I64(mn), _p(mrp), _p(mcol), _p(out))
+    if r != 0:
+        raise ValueError("oracle mxmm: shape mismatch")
+    return out
+
+
+def ktruss(A, k, record=64):
+    m, _, rp, col, _ = _host(A)
+    orp = np.zeros(m + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    nnz = ctypes.c_int64(0)
+    iters = ctypes.c_int(0)
+    per = np.zeros(record, dtype=np.int64)
+    port().orc_ktruss(I64(m), _p(rp), _p(col), ctypes.c_int(k), _p(orp), _p(ocol), ctypes.byref(nnz),
+                      ctypes.byref(iters), _p(per), ctypes.c_int(record))
+    return orp, ocol[: nnz.value].copy(), int(iters.value), per[: min(iters.value, record)].copy()
+
+
+def bc_f64(A, sources):
+    m, _, rp, col, val = _host(A)
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.int32))
+    out = np.zeros(m, dtype=np.float64)
+    port().orc_bc_f64(I64(m), _p(rp), _p(col), _p(val), _p(src), I64(len(src)), _p(out))
+    return out
+
+
+def transpose(A):
+    m, n, rp, col, val = _host(A)
+    orp = np.zeros(n + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    oval = np.zeros(max(len(col), 1), dtype=np.int32)
+    port().orc_transpose(I64(m), I64(n), _p(rp), _p(col), _p(val), _p(orp), _p(ocol), _p(oval))
+    return orp, ocol[: len(col)], oval[: len(col)]
+
+
+def extract_lower(A):
+    m, _, rp, col, _ = _host(A)
+    orp = np.zeros(m + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    nnz = ctypes.c_int64(0)
+    port().orc_extract_lower(I64(m), _p(rp), _p(col), _p(orp), _p(ocol), ctypes.byref(nnz))
+    return orp, ocol[: nnz.value].copy()
+
+
+# ----- reference (compiled reference headers) -----------------------------------
+ACCUM = {"msa": 0, "mca": 1, "naive": 2}
+
+
+def ref_tc(A_sym, accum="msa", parallel=True):
+    m, _, rp, col, _ = _host(A_sym)
+    out = ctypes.c_int64(0)
+    r = ref().ref_tc_sandia(ACCUM[accum], int(parallel), I64(m), _p(rp), _p(col), ctypes.byref(out))
+    if r != 0:
+        raise RuntimeError(f"reference tc failed ({r})")
+    return int(out.value)
+
+
+def ref_tc_rows(L, row_begin, row_end, parallel=True):
+    m, _, rp, col, _ = _host(L)
+    out = ctypes.c_int64(0)
+    r = ref().ref_tc_rows(int(parallel), I64(m), _p(rp), _p(col), I64(row_begin), I64(row_end), ctypes.byref(out))
+    if r != 0:
+        raise RuntimeError(f"reference tc_rows failed ({r})")
+    return int(out.value)
+
+
+def ref_mxmm(A, B, M, accum="msa", parallel=True):
+    am, an, arp, acol, aval = _host(A)
+    bm, bn, brp, bcol, bval = _host(B)
+    mm, mn, mrp, mcol, _ = _host(M)
+    out = np.zeros(int(mrp[-1]), dtype=np.int32)
+    r = ref().ref_mxmm(ACCUM[accum], int(parallel), I64(am), I64(an), _p(arp), _p(acol), _p(aval), I64(bm),
+                       I64(bn), _p(brp), _p(bcol), _p(bval), I64(mm), I64(mn), _p(mrp), _p(mcol), _p(out))
+    if r != 0:
+        raise RuntimeError(f"reference mxmm failed ({r})")
+    return out
+
+
+def ref_ktruss(A_sym, k, accum="msa", parallel=True):
+    m, _, rp, col, _ = _host(A_sym)
+    orp = np.zeros(m + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    nnz = ctypes.c_int64(0)
+    iters = ctypes.c_int(0)
+    r = ref().ref_ktruss(ACCUM[accum], int(parallel), I64(m), _p(rp), _p(col), ctypes.c_int(k), _p(orp), _p(ocol),
+                         ctypes.byref(nnz), ctypes.byref(iters))
+    if r != 0:
+        raise RuntimeError(f"reference ktruss failed ({r})")
+    return orp, ocol[: nnz.value].copy(), int(iters.value)
+
+
+def ref_bc_float(A_sym, b, threads=1):
+    """Reference BC (float, int32 path counts) with sources 0..b-1.  Runs with
+    one OpenMP thread by default: with several threads the reference's row
+    split can leave rows unassigned (include/betweenness_centrality.h:326-332)."""
+    m, _, rp, col, _ = _host(A_sym)
+    out = np.zeros(m, dtype=np.float32)
+    old = ref().ref_get_threads()
+    ref().ref_set_threads(int(threads))
+    try:
+        r = ref().ref_bc_batch(1, I64(m), _p(rp), _p(col), I64(b), _p(out))
+    finally:
+        ref().ref_set_threads(int(old))
+    if r != 0:
+        raise RuntimeError(f"reference bc failed ({r})")
+    return out
+
+
+def ref_transpose(A):
+    m, n, rp, col, val = _host(A)
+    orp = np.zeros(n + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    oval = np.zeros(max(len(col), 1), dtype=np.int32)
+    ref().ref_transpose(I64(m), I64(n), _p(rp), _p(col), _p(val), _p(orp), _p(ocol), _p(oval))
+    return orp, ocol[: len(col)], oval[: len(col)]
+
+
+def ref_extract_lower(A):
+    m, _, rp, col, _ = _host(A)
+    orp = np.zeros(m + 1, dtype=np.int64)
+    ocol = np.zeros(max(len(col), 1), dtype=np.int32)
+    nnz = ctypes.c_int64(0)
+    ref().ref_extract_lower(I64(m), _p(rp), _p(col), _p(orp), _p(ocol), ctypes.byref(nnz))
+    return orp, ocol[: nnz.value].copy()
+
+
+def ref_build_symm(L):
+    m, _, rp, col, _ = _host(L)
+    orp = np.zeros(m + 1, dtype=np.int64)
+    ocol = np.zeros(max(2 * len(col), 1), dtype=np.int32)
+    nnz = ctypes.c_int64(0)
+    ref().ref_build_symm_from_lower(I64(m), _p(rp), _p(col), _p(orp), _p(ocol), ctypes.byref(nnz))
+    return orp, ocol[: nnz.value].copy()
+
+
+def relabel_sources_first(A, sources):
+    """Permutation putting `sources` at labels 0..b-1 (rest in order) and the
+    relabelled symmetric CSR, so that the reference's BC (sources 0..b-1,
+    include/betweenness_centrality.h:445-447) runs on sampled sources."""
+    m, _, rp, col, _ = _host(A)
+    src = np.asarray(sources, dtype=np.int64)
+    perm = np.full(m, -1, dtype=np.int64)  # old -> new
+    perm[src] = np.arange(len(src))
+    # Non-source vertices follow, isolated ones first: the reference's row
+    # split (work_distribution, include/betweenness_centrality.h:326-332)
+    # never assigns trailing empty rows to a team, which leaves stale row
+    # pointers in its frontier and crashes; no trailing empty row avoids it.
+    rest = np.setdiff1d(np.arange(m), src, assume_unique=False)
+    deg = np.diff(rp)[rest]
+    rest = np.concatenate([rest[deg == 0], rest[deg > 0]])
+    perm[rest] = np.arange(len(src), m)
+    rows = np.repeat(np.arange(m), np.diff(rp))
+    nr, nc = perm[rows], perm[col.astype(np.int64)]
+    order = np.lexsort((nc, nr))
+    nr, nc = nr[order], nc[order]
+    nrp = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(np.bincount(nr, minlength=m), out=nrp[1:])
+
+    class _C:
+        pass
+
+    c = _C()
+    c.m = c.n = m
+    c.rowptr, c.col, c.val = nrp, nc.astype(np.int32), None
+    return c, perm

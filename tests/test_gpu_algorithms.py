@@ -1,0 +1,119 @@
+"""Parity of the CUDA k-truss and batched betweenness centrality with the
+oracle: k-truss edge sets bit-exact, FP64 BC within 1e-12 relative."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+BC_RTOL = 1e-12
+
+
+def dev(csr):
+    return csr.to("cuda")
+
+
+@pytest.mark.parametrize("scale,seed,k", [(9, 5, 3), (10, 7, 4), (11, 7, 5), (12, 2, 6), (12, 2, 9)])
+def test_ktruss_matches_oracle(gk, orc, cuda, scale, seed, k):
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    rp, col, iters, _ = orc.ktruss(A, k)
+    T, it = gk.ktruss(dev(A), k)
+    assert it == iters
+    assert T.nnz == len(col)
+    np.testing.assert_array_equal(T.rowptr.cpu().numpy(), rp)
+    np.testing.assert_array_equal(T.col.cpu().numpy(), col)
+
+
+def test_ktruss_host_buffers_and_closed_forms(gk, orc, cuda):
+    T, it = gk.ktruss(G.complete(6), 6)
+    assert T.nnz == 30 and it == 1
+    T, it = gk.ktruss(G.wheel(10), 4)
+    assert T.nnz == 0
+    A = G.from_edges(5, [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (3, 4)])
+    T, it = gk.ktruss(A, 3)
+    assert T.nnz == 12 and it == 2
+    with pytest.raises(gk.GkError):
+        gk.ktruss(A, 2)
+
+
+def test_ktruss_golden(gk, cuda):
+    g = json.load(open(os.path.join(GOLDEN, "ktruss.json")))
+    for case in g["cases"]:
+        A = gk.gen_rmat(case["scale"], case["edge_factor"], seed=case["seed"], device="cuda")
+        T, it = gk.ktruss(A, case["k"])
+        assert it == case["iterations"]
+        assert T.nnz == case["nnz"]
+        rp = T.rowptr.cpu().numpy()
+        col = T.col.cpu().numpy()
+        rows = np.repeat(np.arange(A.m, dtype=np.int64), np.diff(rp))
+        h = int(np.bitwise_xor.reduce((col.astype(np.int64) * 2654435761 + rows) & 0xFFFFFFFF)) if len(col) else 0
+        assert h == case["xor_hash"]
+
+
+def test_ktruss_fixed_point(gk, cuda):
+    A = gk.gen_rmat(12, 16, seed=3, device="cuda")
+    T, _ = gk.ktruss(A, 5)
+    T2, it2 = gk.ktruss(T, 5)
+    assert it2 == 1 and T2.nnz == T.nnz
+
+
+# ---------------------------------------------------------------------------
+# betweenness centrality
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("scale,nsrc,seed", [(9, 40, 1), (10, 64, 2), (11, 100, 3), (12, 512, 4), (10, 1, 5)])
+def test_bc_matches_oracle(gk, orc, cuda, scale, nsrc, seed):
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    rng = np.random.default_rng(seed)
+    src = rng.choice(A.m, size=nsrc, replace=False)
+    want = orc.bc_f64(A, src)
+    got = gk.bc_batch(dev(A), src).cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=BC_RTOL, atol=1e-9)
+
+
+def test_bc_more_than_one_chunk(gk, orc, cuda):
+    A = gk.gen_rmat(10, 8, seed=9)
+    src = np.random.default_rng(1).choice(A.m, size=700, replace=False)
+    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), rtol=BC_RTOL, atol=1e-9)
+
+
+def test_bc_closed_forms_and_host_buffers(gk, cuda):
+    bc = gk.bc_batch(G.path(5), range(5))
+    np.testing.assert_allclose(bc, [0, 6, 8, 6, 0])
+    bc = gk.bc_batch(G.star(6), range(7))
+    assert bc[0] == pytest.approx(30.0) and np.all(bc[1:] == 0)
+
+
+def test_bc_directed(gk, orc, cuda):
+    A = G.random_csr(300, 300, 0.02, seed=11)
+    src = np.arange(0, 300, 7)
+    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), G.brandes_f64(A, src), rtol=BC_RTOL,
+                               atol=1e-9)
+
+
+def test_bc_heavy_vertices(gk, orc, cuda):
+    # hub of degree > 512 goes to the CTA-per-vertex kernels
+    A = G.from_edges(2000, [(0, i) for i in range(1, 2000)] + [(i, i + 1) for i in range(1, 1999, 3)])
+    src = np.arange(0, 2000, 17)
+    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), rtol=BC_RTOL,
+                               atol=1e-9)
+
+
+def test_bc_golden(gk, cuda):
+    g = json.load(open(os.path.join(GOLDEN, "bc.json")))
+    for case in g["cases"]:
+        A = gk.gen_rmat(case["scale"], case["edge_factor"], seed=case["seed"], device="cuda")
+        got = gk.bc_batch(A, case["sources"]).cpu().numpy()
+        np.testing.assert_allclose(got, np.asarray(case["bc_ref_float"]), rtol=2e-4, atol=1e-2)
+
+
+def test_bc_errors(gk, cuda):
+    A = dev(G.path(5))
+    with pytest.raises(gk.GkError):
+        gk.bc_batch(A, [0, 0])
+    with pytest.raises(gk.GkError):
+        gk.bc_batch(A, [7])

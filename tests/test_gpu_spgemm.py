@@ -1,0 +1,211 @@
+"""Parity of the CUDA masked SpGEMM path with the oracle (bit-exact integers).
+
+Every kernel variant is checked on its own (gk_*_variant entry points force
+all rows onto one variant) as well as under the scheduler, on seeded RMAT /
+Erdos-Renyi graphs, random plus-times products with values, hand-made graphs
+and edge cases.  All calls go through the C ABI."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+NV = 10
+
+
+def dev(csr):
+    return csr.to("cuda")
+
+
+@pytest.mark.parametrize("scale,seed", [(8, 1), (10, 2), (12, 3), (14, 1)])
+def test_tc_rmat_every_variant(gk, orc, cuda, scale, seed):
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    L = gk.lower_host(A)
+    want = orc.tc_lower(L)
+    Ld = dev(L)
+    assert gk.tc_count(Ld) == want
+    for v in range(NV):
+        assert gk.tc_count_variant(Ld, v) == want, f"variant {v}"
+
+
+def test_tc_golden_config1(gk, cuda):
+    g = json.load(open(os.path.join(GOLDEN, "tc.json")))
+    case = [c for c in g["cases"] if c["scale"] == 14][0]
+    A = gk.gen_rmat(14, 16, seed=case["seed"], device="cuda")
+    assert A.nnz == case["nnz_sym"]
+    L = gk.extract_lower(A)
+    assert L.nnz == case["nnz_lower"]
+    assert gk.tc_count(L) == case["triangles"]
+    assert gk.tc_count(L, sched="plain") == case["triangles"]
+
+
+def test_tc_host_buffers(gk, orc, cuda):
+    A = gk.gen_rmat(11, 16, seed=4)
+    L = gk.lower_host(A)
+    assert gk.tc_count(L) == orc.tc_lower(L)
+
+
+@pytest.mark.parametrize("maker", [lambda: G.complete(7), lambda: G.wheel(9), lambda: G.star(20),
+                                   lambda: G.path(30), lambda: G.disjoint_triangles(6), lambda: G.empty(5),
+                                   lambda: G.complete(300)])
+def test_tc_small_graphs(gk, orc, cuda, maker):
+    L = gk.lower_host(maker())
+    want = orc.tc_lower(L)
+    Ld = dev(L)
+    assert gk.tc_count(Ld) == want
+    for v in range(NV):
+        assert gk.tc_count_variant(Ld, v) == want
+
+
+def test_tc_er(gk, orc, cuda):
+    A = gk.gen_er(20000, 300000, seed=3)
+    L = gk.lower_host(A)
+    assert gk.tc_count(dev(L)) == orc.tc_lower(L)
+
+
+def test_tc_rmat18(gk, orc, cuda):
+    A = gk.gen_rmat(18, 16, seed=1, device="cuda")
+    L = gk.extract_lower(A)
+    want = orc.tc_lower(L.numpy())
+    assert gk.tc_count(L) == want
+    for v in (0, 3, 5, 6, 9):
+        assert gk.tc_count_variant(L, v) == want
+
+
+def test_tc_row_sums(gk, orc, cuda):
+    A = gk.gen_rmat(12, 16, seed=8)
+    L = gk.lower_host(A)
+    got = gk.tc_row_sums(dev(L)).cpu().numpy().astype(np.uint64)
+    np.testing.assert_array_equal(got, orc.tc_row_sums(L))
+
+
+def test_tc_batched(gk, orc, cuda):
+    graphs = []
+    for i in range(24):
+        if i % 2:
+            A = gk.gen_er(500 + 97 * i, 4000 + 300 * i, seed=100 + i)
+        else:
+            A = gk.gen_rmat(6 + i % 7, 16, seed=100 + i)
+        graphs.append(gk.lower_host(A))
+    want = np.array([orc.tc_lower(L) for L in graphs], dtype=np.uint64)
+    got_host = gk.tc_count_batched(graphs)
+    np.testing.assert_array_equal(got_host, want)
+    got_dev = gk.tc_count_batched([dev(L) for L in graphs])
+    np.testing.assert_array_equal(got_dev, want)
+
+
+# ---------------------------------------------------------------------------
+# general masked SpGEMM with values (plus-times)
+# ---------------------------------------------------------------------------
+CASES = [
+    # (m, k, n, density A, density B, density M)
+    (40, 30, 50, 0.2, 0.2, 0.3),
+    (300, 200, 250, 0.02, 0.05, 0.04),
+    (128, 128, 128, 0.5, 0.5, 0.6),       # long mask rows: chunking in the small variants
+    (600, 400, 3000, 0.01, 0.3, 0.2),     # mask rows of ~600 across a wide column range
+    (1, 5, 7, 1.0, 1.0, 1.0),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mxmm_values_every_variant(gk, orc, cuda, case):
+    m, k, n, da, db, dm = case
+    A = G.random_csr(m, k, da, 1, values=True)
+    B = G.random_csr(k, n, db, 2, values=True)
+    M = G.random_csr(m, n, dm, 3)
+    want = orc.mxmm(A, B, M)
+    Ad, Bd, Md = dev(A), dev(B), dev(M)
+    for v in range(NV):
+        got = gk.mxmm_masked_variant(Ad, Bd, Md, v).cpu().numpy()
+        np.testing.assert_array_equal(got, want, err_msg=f"variant {v}")
+    for accum in ("auto", "msa", "mca", "hash"):
+        got = gk.mxmm_masked(Ad, Bd, Md, accum=accum).cpu().numpy()
+        np.testing.assert_array_equal(got, want, err_msg=accum)
+    # host buffers through the same entry point
+    np.testing.assert_array_equal(gk.mxmm_masked(A, B, M), want)
+
+
+def test_mxmm_plus_pair(gk, orc, cuda):
+    A = G.random_csr(200, 150, 0.05, 4, values=True)
+    B = G.random_csr(150, 180, 0.05, 5, values=True)
+    M = G.random_csr(200, 180, 0.1, 6)
+    import copy
+    Ap, Bp = copy.copy(A), copy.copy(B)
+    Ap.val = None
+    Bp.val = None
+    want = orc.mxmm(Ap, Bp, M)
+    got = gk.mxmm_masked(dev(A), dev(B), dev(M), semiring="plus_pair").cpu().numpy()
+    np.testing.assert_array_equal(got, want)
+
+
+def test_mxmm_edge_cases(gk, orc, cuda):
+    # empty A rows, empty mask rows, empty B, zero-size shapes
+    A = G.random_csr(50, 40, 0.05, 7, values=True)
+    B = G.empty(40)
+    B = type(B)(40, 60, np.zeros(41, dtype=np.int64), np.zeros(0, dtype=np.int32), None, 0)
+    M = G.random_csr(50, 60, 0.2, 8)
+    got = gk.mxmm_masked(dev(A), dev(B), dev(M)).cpu().numpy()
+    assert np.all(got == 0) and len(got) == M.nnz
+    Z = G.empty(0)
+    assert len(gk.mxmm_masked(Z, Z, Z)) == 0
+    with pytest.raises(gk.GkError) as e:
+        gk.mxmm_masked(dev(A), dev(A), dev(M))
+    assert e.value.code == 1
+
+
+def test_mxmm_square_graph(gk, orc, cuda):
+    A = gk.gen_rmat(11, 16, seed=21)
+    want = orc.mxmm(A, A, A)
+    Ad = dev(A)
+    for v in range(NV):
+        np.testing.assert_array_equal(gk.mxmm_masked_variant(Ad, Ad, Ad, v, semiring="plus_pair").cpu().numpy(),
+                                      want, err_msg=f"variant {v}")
+
+
+# ---------------------------------------------------------------------------
+# graph ingest on the device
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("scale,seed", [(6, 1), (10, 7), (14, 2), (16, 3)])
+def test_device_rmat_equals_host(gk, cuda, scale, seed):
+    H = gk.gen_rmat(scale, 16, seed=seed)
+    D = gk.gen_rmat(scale, 16, seed=seed, device="cuda")
+    assert D.nnz == H.nnz
+    np.testing.assert_array_equal(D.rowptr.cpu().numpy(), H.rowptr)
+    np.testing.assert_array_equal(D.col.cpu().numpy(), H.col)
+
+
+def test_device_er_equals_host(gk, cuda):
+    H = gk.gen_er(12345, 100000, seed=77)
+    D = gk.gen_er(12345, 100000, seed=77, device="cuda")
+    np.testing.assert_array_equal(D.rowptr.cpu().numpy(), H.rowptr)
+    np.testing.assert_array_equal(D.col.cpu().numpy(), H.col)
+
+
+def test_device_transforms(gk, orc, cuda):
+    A = gk.gen_rmat(12, 8, seed=5)
+    L = gk.extract_lower(dev(A))
+    orp, ocol = orc.extract_lower(A)
+    np.testing.assert_array_equal(L.rowptr.cpu().numpy(), orp)
+    np.testing.assert_array_equal(L.col.cpu().numpy(), ocol)
+    R = G.random_csr(300, 500, 0.02, 9, values=True)
+    T = gk.transpose(dev(R), with_values=True)
+    trp, tcol, tval = orc.transpose(R)
+    np.testing.assert_array_equal(T.rowptr.cpu().numpy(), trp)
+    np.testing.assert_array_equal(T.col.cpu().numpy(), tcol)
+    np.testing.assert_array_equal(T.val.cpu().numpy(), tval)
+    Th = gk.transpose(R, with_values=True)  # host buffers
+    np.testing.assert_array_equal(Th.col, tcol)
+
+
+def test_learned_without_model_is_an_error(gk, cuda):
+    if gk.load().gk_sched_has_model():
+        pytest.skip("a model is loaded in this process")
+    L = dev(gk.lower_host(G.complete(5)))
+    with pytest.raises(gk.GkError) as e:
+        gk.tc_count(L, sched="learned")
+    assert e.value.code == 1

@@ -1,0 +1,226 @@
+"""Pins the oracle (CPU restatement, oracle/gk_oracle.cpp) to the reference.
+
+Three kinds of evidence, as the reference ships no test vectors:
+  * the reference's own code, compiled unmodified against the Kokkos-API shim
+    (oracle/_ref), run on the same seeded inputs (skipped where it was not
+    built);
+  * golden fixtures generated from that build (tests/golden/, made by
+    tests/golden/make_golden.py);
+  * closed-form answers on hand-made graphs and independent second methods.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests import graphs as G
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def need_ref(orc):
+    if not orc.ref_available():
+        pytest.skip("reference oracle not built (reference sources absent)")
+
+
+# ---------------------------------------------------------------------------
+# closed forms
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n,tri", [(3, 1), (4, 4), (5, 10), (8, 56)])
+def test_tc_complete(gk, orc, n, tri):
+    L = gk.lower_host(G.complete(n))
+    assert orc.tc_lower(L) == tri
+    assert orc.tc_merge(L) == tri
+
+
+def test_tc_shapes(gk, orc):
+    assert orc.tc_lower(gk.lower_host(G.wheel(7))) == 7
+    assert orc.tc_lower(gk.lower_host(G.star(9))) == 0
+    assert orc.tc_lower(gk.lower_host(G.path(10))) == 0
+    assert orc.tc_lower(gk.lower_host(G.disjoint_triangles(5))) == 5
+    assert orc.tc_lower(gk.lower_host(G.empty(6))) == 0
+
+
+def test_ktruss_closed_forms(orc):
+    # K5 is a 5-truss (every edge in 3 triangles); a wheel's rim edges have support 1
+    rp, col, iters, _ = orc.ktruss(G.complete(5), 5)
+    assert len(col) == 20 and iters == 1
+    rp, col, iters, _ = orc.ktruss(G.wheel(8), 4)
+    assert len(col) == 0
+    # K4 plus a pendant edge: the pendant has support 0 and is removed for k=3
+    A = G.from_edges(5, [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3), (3, 4)])
+    rp, col, iters, _ = orc.ktruss(A, 3)
+    assert len(col) == 12 and iters == 2
+
+
+def test_bc_closed_forms(orc):
+    # path 0-1-2-3-4, all sources: bc(v) = 2 * (#pairs separated by v)
+    P = G.path(5)
+    bc = orc.bc_f64(P, range(5))
+    np.testing.assert_allclose(bc, [0, 6, 8, 6, 0])
+    # star with 6 leaves, all sources: hub = 6*5
+    bc = orc.bc_f64(G.star(6), range(7))
+    assert bc[0] == pytest.approx(30.0)
+    assert np.all(bc[1:] == 0)
+
+
+def test_bc_matches_brandes(gk, orc):
+    A = gk.gen_rmat(9, 8, seed=11)
+    rng = np.random.default_rng(3)
+    src = rng.choice(A.m, size=40, replace=False)
+    ours = orc.bc_f64(A, src)
+    ref = G.brandes_f64(A, src)
+    np.testing.assert_allclose(ours, ref, rtol=1e-12, atol=1e-9)
+
+
+def test_bc_directed_matches_brandes(orc):
+    A = G.random_csr(60, 60, 0.06, seed=5)
+    src = np.arange(0, 60, 3)
+    np.testing.assert_allclose(orc.bc_f64(A, src), G.brandes_f64(A, src), rtol=1e-12, atol=1e-9)
+
+
+def test_mxmm_dense(orc):
+    for seed in range(4):
+        A = G.random_csr(37, 23, 0.2, seed, values=True)
+        B = G.random_csr(23, 41, 0.25, seed + 10, values=True)
+        M = G.random_csr(37, 41, 0.3, seed + 20)
+        c = orc.mxmm(A, B, M)
+        full = G.dense_of(A) @ G.dense_of(B)
+        rp, col = M.rowptr, M.col
+        want = np.concatenate([full[i, col[rp[i]:rp[i + 1]]] for i in range(M.m)])
+        np.testing.assert_array_equal(c, want.astype(np.int32))
+
+
+def test_transforms(gk, orc):
+    A = gk.gen_rmat(8, 8, seed=4)
+    orp, ocol = orc.extract_lower(A)
+    L = gk.lower_host(A)
+    np.testing.assert_array_equal(orp, L.rowptr)
+    np.testing.assert_array_equal(ocol, L.col)
+    trp, tcol, _ = orc.transpose(A)
+    np.testing.assert_array_equal(trp, A.rowptr)  # symmetric
+    np.testing.assert_array_equal(tcol, A.col)
+
+
+# ---------------------------------------------------------------------------
+# against the reference's own code
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("scale,seed", [(8, 1), (10, 2), (12, 3)])
+def test_tc_vs_reference(gk, orc, scale, seed):
+    need_ref(orc)
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    L = gk.lower_host(A)
+    got = orc.tc_lower(L)
+    for accum in ("msa", "mca"):
+        assert orc.ref_tc(A, accum) == got
+    # the sequential MCA agrees too; the sequential MSA (matrix_la.h:696-731)
+    # does not reset its value array between rows, so its explicit zeros can
+    # carry stale values from earlier rows (a reference defect, not tested)
+    assert orc.ref_tc(A, "mca", parallel=False) == got
+
+
+def test_mxmm_vs_reference(gk, orc):
+    need_ref(orc)
+    for seed in range(3):
+        A = G.random_csr(120, 90, 0.05, seed, values=True)
+        B = G.random_csr(90, 110, 0.06, seed + 1, values=True)
+        M = G.random_csr(120, 110, 0.08, seed + 2)
+        want = orc.mxmm(A, B, M)
+        for accum in ("msa", "mca"):
+            np.testing.assert_array_equal(orc.ref_mxmm(A, B, M, accum), want)
+        np.testing.assert_array_equal(orc.ref_mxmm(A, B, M, "naive", parallel=False), want)
+
+
+@pytest.mark.parametrize("k", [3, 4, 5, 6])
+def test_ktruss_vs_reference(gk, orc, k):
+    need_ref(orc)
+    A = gk.gen_rmat(10, 16, seed=7)
+    rp, col, iters, _ = orc.ktruss(A, k)
+    rrp, rcol, riters = orc.ref_ktruss(A, k)
+    np.testing.assert_array_equal(rp, rrp)
+    np.testing.assert_array_equal(col, rcol)
+    assert iters == riters
+
+
+def test_transforms_vs_reference(gk, orc):
+    need_ref(orc)
+    A = gk.gen_rmat(9, 8, seed=9)
+    rrp, rcol = orc.ref_extract_lower(A)
+    orp, ocol = orc.extract_lower(A)
+    np.testing.assert_array_equal(rrp, orp)
+    np.testing.assert_array_equal(rcol, ocol)
+    L = gk.lower_host(A)
+    srp, scol = orc.ref_build_symm(L)
+    np.testing.assert_array_equal(srp, A.rowptr)
+    np.testing.assert_array_equal(scol, A.col)
+    D = G.random_csr(50, 70, 0.1, seed=3, values=True)
+    a = orc.ref_transpose(D)
+    b = orc.transpose(D)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_bc_vs_reference_float(gk, orc):
+    """The reference BC is FP32 with int32 path counts; on a graph where no
+    count overflows it must agree with the FP64 restatement to float precision.
+    Sampled sources are relabelled to 0..b-1 (the reference's only sources)."""
+    need_ref(orc)
+    A = gk.gen_rmat(10, 8, seed=12)
+    rng = np.random.default_rng(4)
+    src = rng.choice(A.m, size=64, replace=False)
+    ours = orc.bc_f64(A, src)
+    R, perm = orc.relabel_sources_first(A, src)
+    ref = orc.ref_bc_float(R, len(src))
+    ref_orig = ref[perm]
+    np.testing.assert_allclose(ref_orig, ours, rtol=2e-4, atol=1e-2)
+
+
+# ---------------------------------------------------------------------------
+# golden fixtures (generated from the reference build; valid without it)
+# ---------------------------------------------------------------------------
+def _golden(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+def test_golden_tc(gk, orc):
+    g = _golden("tc.json")
+    for case in g["cases"]:
+        A = gk.gen_rmat(case["scale"], case["edge_factor"], seed=case["seed"])
+        assert A.nnz == case["nnz_sym"]
+        L = gk.lower_host(A)
+        assert L.nnz == case["nnz_lower"]
+        assert orc.tc_lower(L) == case["triangles"]
+
+
+def test_golden_ktruss(gk, orc):
+    g = _golden("ktruss.json")
+    for case in g["cases"]:
+        A = gk.gen_rmat(case["scale"], case["edge_factor"], seed=case["seed"])
+        rp, col, iters, _ = orc.ktruss(A, case["k"])
+        assert iters == case["iterations"]
+        assert len(col) == case["nnz"]
+        assert int(np.bitwise_xor.reduce((col.astype(np.int64) * 2654435761 + np.repeat(
+            np.arange(A.m), np.diff(rp))) & 0xFFFFFFFF)) == case["xor_hash"]
+
+
+def test_golden_mxmm(orc):
+    g = _golden("mxmm.json")
+    for case in g["cases"]:
+        A = G.random_csr(*case["A"], values=True)
+        B = G.random_csr(*case["B"], values=True)
+        M = G.random_csr(*case["M"])
+        c = orc.mxmm(A, B, M)
+        assert int(c.astype(np.int64).sum()) == case["sum"]
+        assert int((c.astype(np.int64) * np.arange(1, len(c) + 1)).sum()) == case["weighted_sum"]
+
+
+def test_golden_bc(gk, orc):
+    g = _golden("bc.json")
+    for case in g["cases"]:
+        A = gk.gen_rmat(case["scale"], case["edge_factor"], seed=case["seed"])
+        src = np.asarray(case["sources"])
+        ours = orc.bc_f64(A, src)
+        ref = np.asarray(case["bc_ref_float"], dtype=np.float64)
+        np.testing.assert_allclose(ours, ref, rtol=2e-4, atol=1e-2)
