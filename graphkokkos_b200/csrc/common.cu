@@ -167,33 +167,51 @@ ProfWindow::~ProfWindow() {
     }
 }
 
-void ProfWindow::begin(int slot) {
+void ProfWindow::begin(int slot, cudaStream_t on) {
     if (events_only_) {
         Pending p{slot, nullptr, nullptr};
         cudaEventCreate(&p.a);
         cudaEventCreate(&p.b);
-        cudaEventRecord(p.a, s_);
+        cudaEventRecord(p.a, on);
         std::lock_guard<std::mutex> lock(g_prof_mutex);
         g_pending.push_back(p);
         return;
     }
-    if (on_ && slot < slots_) cudaEventRecord(ev_[slot][0], s_);
+    if (on_ && slot < slots_) cudaEventRecord(ev_[slot][0], on);
 }
 
-void ProfWindow::end(int slot) {
+void ProfWindow::end(int slot, cudaStream_t on) {
     if (events_only_) {
         std::lock_guard<std::mutex> lock(g_prof_mutex);
         for (auto it = g_pending.rbegin(); it != g_pending.rend(); ++it)
             if (it->variant == slot) {
-                cudaEventRecord(it->b, s_);
+                cudaEventRecord(it->b, on);
                 break;
             }
         return;
     }
     if (on_ && slot < slots_) {
-        cudaEventRecord(ev_[slot][1], s_);
+        cudaEventRecord(ev_[slot][1], on);
         used_[slot] = true;
     }
+}
+
+SideStreams &side_streams() {
+    static thread_local SideStreams per_dev[16];
+    static thread_local bool ready[16] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    dev &= 15;
+    if (!ready[dev]) {
+        SideStreams &x = per_dev[dev];
+        for (int i = 0; i < 16; ++i) {
+            cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking);
+            cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming);
+        }
+        cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming);
+        ready[dev] = true;
+    }
+    return per_dev[dev];
 }
 
 int ProfWindow::finish(const ProfTotals *totals) {

@@ -79,6 +79,16 @@ int validate_csr_shape(const gk_csr *c, const char *name);
 
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
+// ----- side streams for concurrent kernel variants ----------------------------
+// Non-blocking streams and fork/join events, one set per host thread and
+// device, so that concurrent callers never share an event.
+struct SideStreams {
+    cudaStream_t s[16];
+    cudaEvent_t fork;
+    cudaEvent_t join[16];
+};
+SideStreams &side_streams();
+
 // ----- launch counter and per-variant profiling (gk_launch_count, gk_prof_*) ----
 void note_launches(int n);
 bool prof_enabled();
@@ -94,8 +104,8 @@ public:
     ProfWindow(cudaStream_t s, int slots);
     ~ProfWindow();
     bool active() const { return on_; }
-    void begin(int slot);
-    void end(int slot);
+    void begin(int slot, cudaStream_t on);
+    void end(int slot, cudaStream_t on);
     int finish(const ProfTotals *totals);
 
 private:

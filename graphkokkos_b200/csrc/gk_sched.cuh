@@ -35,6 +35,7 @@ enum Kind : int { K_HASH_GROUP = 0, K_HASH_BLOCK = 1, K_MCA_GROUP = 2, K_MCA_BLO
 struct Variant {
     int kind;
     int G;          // threads per row (group kinds) or per CTA (block kinds)
+    int sub;        // lanes that stream one B row together (G/sub rows of B in flight per row)
     int cap;        // hash slots (HASH), sorted slots (MCA), log2 window columns (MSA)
     int cap_write;  // same when values are written back (WRITE epilogue needs accumulators)
     int chunk;      // mask entries per item (HASH/MCA); unused by MSA
@@ -43,27 +44,32 @@ struct Variant {
     int accum;      // gk_accum family this variant belongs to
 };
 
-constexpr int NV = 10;
+constexpr int NV = 13;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
-// columns: kind, G, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, accum family
+// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, accum family
 #define GK_VARIANT_TABLE { \
-    {K_HASH_GROUP,   4,    64,    64,    16,    16,   0, 3},   \
-    {K_HASH_GROUP,   8,   128,   128,    32,    32,   0, 3},   \
-    {K_HASH_GROUP,  16,   256,   256,    64,    64,   0, 3},   \
-    {K_HASH_GROUP,  32,   512,   512,   128,   128,   0, 3},   \
-    {K_HASH_GROUP,  32,  2048,  2048,   512,   512,   0, 3},   \
-    {K_HASH_BLOCK, 256,  8192,  8192,  4096,  4096,  20, 3},   \
-    {K_HASH_BLOCK, 512, 32768, 16384, 16384,  8192,  22, 3},   \
-    {K_MCA_GROUP,   32,   256,   256,   256,   256,   0, 2},   \
-    {K_MCA_BLOCK,  512, 16384, 16384, 16384, 16384,  22, 2},   \
-    {K_MSA_BLOCK,  512,    20,    15,     0,     0,  22, 1},   \
+    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0, 3},   \
+    {K_HASH_GROUP,   8,  4,   128,   128,    32,    32,   0, 3},   \
+    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0, 3},   \
+    {K_HASH_GROUP,  16,  4,   256,   256,    64,    64,   0, 3},   \
+    {K_HASH_GROUP,  16, 16,   256,   256,    64,    64,   0, 3},   \
+    {K_HASH_GROUP,  32,  8,   512,   512,   128,   128,   0, 3},   \
+    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 3},   \
+    {K_HASH_GROUP,  32, 16,  2048,  2048,   512,   512,   0, 3},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  18, 3},   \
+    {K_HASH_BLOCK, 512, 32, 32768, 16384, 16384,  8192,  20, 3},   \
+    {K_MCA_GROUP,   32,  8,   256,   256,   256,   256,   0, 2},   \
+    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20, 2},   \
+    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20, 1},   \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
 __constant__ const Variant c_variants[NV] = GK_VARIANT_TABLE;  // runtime-indexed copy for device code
 #endif
-constexpr int NT_GROUP = 256;  // CTA size of the group kinds (variant 4 uses 128)
-__host__ __device__ constexpr int group_cta_threads(int v) { return v == 4 ? 128 : NT_GROUP; }
+constexpr int NT_GROUP = 256;  // CTA size of the group kinds (variant 7 uses 128)
+__host__ __device__ constexpr int group_cta_threads(int v) { return v == 7 ? 128 : NT_GROUP; }
+// variant ids the heuristics name
+constexpr int V_MCA_GROUP = 10, V_MCA_BLOCK = 11, V_MSA_BLOCK = 12;
 
 // ---- features of a bin (inputs of the learned scheduler) ---------------------
 constexpr int NFEAT = 8;

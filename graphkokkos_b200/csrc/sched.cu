@@ -44,27 +44,25 @@ __host__ __device__ inline void bin_features(const BinStats &b, int epi, bool va
 // chunk, a wider thread group when the streamed B rows are long, and a block
 // kind (which splits rows over CTAs) when a row carries a lot of work.
 __host__ __device__ inline int plain_variant(int bin, const BinStats &b) {
-    const int qm = bin / NB_B, qb = bin % NB_B;
+    const int qm = bin / NB_B, qb = bin % NB_B;  // log2 mask-row length, log2 mean B-row length
     int v;
-    if (qm <= 3) v = 0;
-    else if (qm == 4) v = 1;
-    else if (qm == 5) v = 2;
-    else if (qm == 6) v = 3;
-    else if (qm <= 8) v = 4;
-    else if (qm <= 11) v = 5;
-    else v = 6;
-    if (v <= 1 && qb >= 4) v = 2;
-    if (v <= 2 && qb >= 6) v = 3;
+    if (qm <= 3) v = qb <= 3 ? 0 : (qb <= 6 ? 3 : 5);       // < 16 mask entries
+    else if (qm == 4) v = qb <= 4 ? 1 : (qb <= 6 ? 3 : 5);  // < 32
+    else if (qm == 5) v = qb <= 6 ? 3 : 5;                  // < 64
+    else if (qm == 6) v = qb <= 8 ? 5 : 6;                  // < 128
+    else if (qm <= 8) v = 7;                                // < 512
+    else if (qm <= 11) v = 8;                               // < 4096
+    else v = 9;
     const double mean_w = static_cast<double>(b.sum_work) / static_cast<double>(b.rows ? b.rows : 1);
-    if (v <= 4 && mean_w > double(1 << 21)) v = 5;
+    if (v <= 7 && mean_w > double(1 << 21)) v = 8;  // heavy rows: split over CTAs
     return v;
 }
 
 __host__ __device__ inline int forced_variant(int bin, const BinStats &b, int accum) {
     const int qm = bin / NB_B;
     switch (accum) {
-        case GK_ACCUM_MSA: return 9;
-        case GK_ACCUM_MCA: return qm <= 7 ? 7 : 8;
+        case GK_ACCUM_MSA: return V_MSA_BLOCK;
+        case GK_ACCUM_MCA: return qm <= 7 ? V_MCA_GROUP : V_MCA_BLOCK;
         default: return plain_variant(bin, b);
     }
 }

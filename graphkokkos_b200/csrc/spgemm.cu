@@ -53,37 +53,6 @@ struct KArgs {
 };
 
 // ---------------------------------------------------------------------------
-// streaming helper: calls probe(x, b) for every element of B_k[b0, b1)
-// handled by this lane (lanes of a group of G stride the row).
-// ---------------------------------------------------------------------------
-template <int G, bool VAL, class F>
-__device__ __forceinline__ void stream_brow(const KArgs &p, int64_t b0, int64_t b1, int lane, F &&probe) {
-    const int32_t *__restrict__ bc = p.B.col;
-    if (!VAL && p.vec) {
-        int64_t h1 = (b0 + 3) & ~int64_t(3);
-        if (h1 > b1) h1 = b1;
-        if (b0 + lane < h1) probe(__ldg(bc + b0 + lane), 1u);
-        const int64_t v0 = h1 >> 2, v1 = b1 >> 2;
-        const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
-#pragma unroll 2
-        for (int64_t q = v0 + lane; q < v1; q += G) {
-            const int4 x = __ldg(bv + q);
-            probe(x.x, 1u);
-            probe(x.y, 1u);
-            probe(x.z, 1u);
-            probe(x.w, 1u);
-        }
-        int64_t tl = v1 << 2;
-        if (tl < h1) tl = h1;
-        if (tl + lane < b1) probe(__ldg(bc + tl + lane), 1u);
-    } else {
-        const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
-        for (int64_t j = b0 + lane; j < b1; j += G)
-            probe(__ldg(bc + j), (VAL && bvals) ? static_cast<uint32_t>(__ldg(bvals + j)) : 1u);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // plan kernels
 // ---------------------------------------------------------------------------
 __global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
@@ -228,14 +197,134 @@ __global__ void k_scatter_rows(DevCsr A, DevCsr M, const int64_t *work, const ui
 // ---------------------------------------------------------------------------
 // group kinds: one row per group of G threads
 // ---------------------------------------------------------------------------
-template <int G, int NT, int CAP, int CHUNK, bool MCA, int EPI, bool VAL>
+// Probe kinds: the mask structure a B-row element is looked up in.
+enum : int { PK_HASH = 0, PK_MCA = 1, PK_MSA = 2 };
+
+// One B-row element against the mask structure of the current row/chunk:
+// HASH  slot of x in a CAP-slot hash set;  MCA  position of x in the sorted
+// chunk keys[0, clen);  MSA  x - base if its bit is set in a 2^CAP-column
+// window bitmap (keys reinterpreted as words).
+template <int CAP, int PK, bool ACC>
+__device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, int *acc, int clen, unsigned &cnt) {
+    int s;
+    if constexpr (PK == PK_MSA) {
+        const int y = x - clen;  // clen carries the window base for MSA
+        s = (y >= 0 && y < (1 << CAP) && ((reinterpret_cast<const unsigned *>(keys)[y >> 5] >> (y & 31)) & 1u)) ? y : -1;
+    } else if constexpr (PK == PK_MCA) {
+        s = sorted_find(keys, clen, x);
+    } else {
+        s = hash_find<CAP>(keys, x);
+    }
+    if (s >= 0) {
+        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), w);
+        else cnt += w;
+    }
+}
+
+// The SUB lanes of a sub-group stream B[b0, b1): 16-byte vector loads, two in
+// flight per lane, scalar head/tail; with values, scalar loads of col and val.
+template <int SUB, int CAP, int PK, bool ACC, bool VAL>
+__device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b1, int sl, uint32_t av,
+                                           const int *keys, int *acc, int clen, unsigned &cnt) {
+    const int32_t *__restrict__ bc = p.B.col;
+    if (!VAL && p.vec) {
+        int64_t h1 = (b0 + 3) & ~int64_t(3);
+        if (h1 > b1) h1 = b1;
+        if (b0 + sl < h1) probe_elem<CAP, PK, ACC>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt);
+        const int64_t v1 = b1 >> 2;
+        const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
+        int64_t q = (h1 >> 2) + sl;
+        for (; q + SUB < v1; q += 2 * SUB) {
+            const int4 x = __ldg(bv + q);
+            const int4 y = __ldg(bv + q + SUB);
+            probe_elem<CAP, PK, ACC>(x.x, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.y, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.z, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.w, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(y.x, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(y.y, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(y.z, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(y.w, av, keys, acc, clen, cnt);
+        }
+        if (q < v1) {
+            const int4 x = __ldg(bv + q);
+            probe_elem<CAP, PK, ACC>(x.x, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.y, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.z, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC>(x.w, av, keys, acc, clen, cnt);
+        }
+        int64_t tl = v1 << 2;
+        if (tl < h1) tl = h1;
+        if (tl + sl < b1) probe_elem<CAP, PK, ACC>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt);
+    } else {
+        const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
+        for (int64_t j = b0 + sl; j < b1; j += SUB) {
+            const uint32_t w = (VAL && bvals) ? av * static_cast<uint32_t>(__ldg(bvals + j)) : av;
+            probe_elem<CAP, PK, ACC>(__ldg(bc + j), w, keys, acc, clen, cnt);
+        }
+    }
+}
+
+// Row bounds of B_k for A entry t (b0 == b1 when outside [lo_col, hi_col]).
+struct BRow {
+    int64_t b0, b1;
+    uint32_t av;
+};
+
+template <bool VAL>
+__device__ __forceinline__ BRow brow_of(const KArgs &p, int k, int64_t t) {
+    BRow r;
+    r.b0 = __ldg(p.B.rp + k);
+    r.b1 = __ldg(p.B.rp + k + 1);
+    r.av = (VAL && p.A.val) ? static_cast<uint32_t>(__ldg(p.A.val + t)) : 1u;
+    return r;
+}
+
+// Streams the B rows of A entries t = first, first+step, ... < a1 with one
+// sub-group of SUB lanes: the next entry's row bounds and the entry after
+// that's column are loaded while the current row streams.
+template <int SUB, int CAP, int PK, bool ACC, bool VAL>
+__device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, int64_t a1, int step, int sl,
+                                               bool chunked, int lo_col, int hi_col, const int *keys, int *acc,
+                                               int clen, unsigned &cnt) {
+    const unsigned smask = group_mask<SUB>();
+    int64_t t = first;
+    if (t >= a1) return;
+    BRow nxt = brow_of<VAL>(p, __ldg(p.A.col + t), t);
+    int k2 = (t + step < a1) ? __ldg(p.A.col + t + step) : 0;
+    while (t < a1) {
+        BRow cur = nxt;
+        const int64_t tn = t + step;
+        if (tn < a1) nxt = brow_of<VAL>(p, k2, tn);
+        if (tn + step < a1) k2 = __ldg(p.A.col + tn + step);
+        if (cur.b0 < cur.b1) {
+            bool skip = false;
+            if (chunked) {
+                skip = __ldg(p.B.col + cur.b1 - 1) < lo_col || __ldg(p.B.col + cur.b0) > hi_col;
+                if (!skip) {
+                    const int64_t lo = group_lower_bound<SUB>(p.B.col, cur.b0, cur.b1, lo_col, sl, smask);
+                    cur.b1 = group_lower_bound<SUB>(p.B.col, lo, cur.b1, hi_col + 1, sl, smask);
+                    cur.b0 = lo;
+                }
+            }
+            if (!skip) stream_row<SUB, CAP, PK, ACC, VAL>(p, cur.b0, cur.b1, sl, cur.av, keys, acc, clen, cnt);
+        }
+        t = tn;
+    }
+}
+
+// G threads per row; the row's A entries are dealt round-robin to G/SUB
+// sub-groups of SUB lanes that stream their B rows concurrently.
+template <int G, int SUB, int NT, int CAP, int CHUNK, bool MCA, int EPI, bool VAL>
 __global__ void __launch_bounds__(NT) k_group(KArgs p) {
     constexpr int NG = NT / G;
+    constexpr int S = G / SUB;
     constexpr bool ACC = (EPI == EPI_WRITE);
     extern __shared__ int smem[];
     __shared__ unsigned long long s_red[NT / 32];
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
+    const int sg = lane / SUB, sl = lane % SUB;
     int *keys = smem + g * CAP;
     int *acc = smem + NG * CAP + g * CAP;
     const unsigned gmask = group_mask<G>();
@@ -269,24 +358,8 @@ __global__ void __launch_bounds__(NT) k_group(KArgs p) {
             __syncwarp(gmask);
             const int lo_col = mc[c0], hi_col = mc[c1 - 1];
             unsigned cnt = 0;
-            for (int64_t t = a0; t < a1; ++t) {
-                const int k = __ldg(p.A.col + t);
-                const uint32_t av = (VAL && p.A.val) ? static_cast<uint32_t>(__ldg(p.A.val + t)) : 1u;
-                int64_t b0 = __ldg(p.B.rp + k), b1 = __ldg(p.B.rp + k + 1);
-                if (b0 >= b1) continue;
-                if (chunked) {
-                    if (__ldg(p.B.col + b1 - 1) < lo_col || __ldg(p.B.col + b0) > hi_col) continue;
-                    b0 = group_lower_bound<G>(p.B.col, b0, b1, lo_col, lane, gmask);
-                    b1 = group_lower_bound<G>(p.B.col, b0, b1, hi_col + 1, lane, gmask);
-                }
-                stream_brow<G, VAL>(p, b0, b1, lane, [&](int x, uint32_t bv) {
-                    const int s = MCA ? sorted_find(keys, clen, x) : hash_find<CAP>(keys, x);
-                    if (s >= 0) {
-                        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), av * bv);
-                        else cnt += av * bv;
-                    }
-                });
-            }
+            stream_entries<SUB, CAP, MCA ? PK_MCA : PK_HASH, ACC, VAL>(p, a0 + sg, a1, S, sl, chunked, lo_col,
+                                                                       hi_col, keys, acc, clen, cnt);
             if (ACC) {
                 __syncwarp(gmask);
                 for (int q = c0 + lane; q < c1; q += G) {
@@ -408,40 +481,47 @@ __global__ void __launch_bounds__(NT) k_block(KArgs p) {
         if (threadIdx.x == 0) s_next = static_cast<int>(0);
         __syncthreads();
 
-        // ---- stream the B rows of A entries [t0, t1), one entry per warp at a time ----
+        // ---- stream the B rows of A entries [t0, t1); warps fetch entries
+        //      dynamically, the next entry's bounds load during the current row ----
         unsigned cnt = 0;
         const int clen = c1 - c0;
         if (c1 > c0) {
-            while (true) {
+            constexpr int PKV = (KIND == K_MSA_BLOCK) ? PK_MSA : ((KIND == K_MCA_BLOCK) ? PK_MCA : PK_HASH);
+            const int probe_arg = (KIND == K_MSA_BLOCK) ? lo_col : clen;
+            const int *pkeys = (KIND == K_MSA_BLOCK) ? reinterpret_cast<const int *>(bits) : keys;
+            auto fetch = [&]() -> int64_t {
                 int tt = 0;
                 if (lane == 0) tt = atomicAdd(&s_next, 1);
-                tt = __shfl_sync(0xFFFFFFFFu, tt, 0);
-                const int64_t t = t0 + tt;
-                if (t >= t1) break;
-                const int k = __ldg(p.A.col + t);
-                const uint32_t av = (VAL && p.A.val) ? static_cast<uint32_t>(__ldg(p.A.val + t)) : 1u;
-                int64_t b0 = __ldg(p.B.rp + k), b1 = __ldg(p.B.rp + k + 1);
-                if (b0 >= b1) continue;
-                if (__ldg(p.B.col + b1 - 1) < lo_col || __ldg(p.B.col + b0) > hi_col) continue;
-                if (cut) {
-                    b0 = group_lower_bound<32>(p.B.col, b0, b1, lo_col, lane, 0xFFFFFFFFu);
-                    b1 = group_lower_bound<32>(p.B.col, b0, b1, hi_col + 1, lane, 0xFFFFFFFFu);
+                return t0 + __shfl_sync(0xFFFFFFFFu, tt, 0);
+            };
+            int64_t tc = fetch();
+            if (tc < t1) {
+                BRow nxt = brow_of<VAL>(p, __ldg(p.A.col + tc), tc);
+                int64_t tn = fetch();
+                int k2 = tn < t1 ? __ldg(p.A.col + tn) : 0;
+                while (tc < t1) {
+                    BRow cur = nxt;
+                    if (tn < t1) nxt = brow_of<VAL>(p, k2, tn);
+                    const int64_t tnn = (tn < t1) ? fetch() : t1;
+                    if (tnn < t1) k2 = __ldg(p.A.col + tnn);
+                    if (cur.b0 < cur.b1) {
+                        bool skip = false;
+                        if (cut) {
+                            skip = __ldg(p.B.col + cur.b1 - 1) < lo_col || __ldg(p.B.col + cur.b0) > hi_col;
+                            if (!skip) {
+                                const int64_t lo = group_lower_bound<32>(p.B.col, cur.b0, cur.b1, lo_col, lane,
+                                                                         0xFFFFFFFFu);
+                                cur.b1 = group_lower_bound<32>(p.B.col, lo, cur.b1, hi_col + 1, lane, 0xFFFFFFFFu);
+                                cur.b0 = lo;
+                            }
+                        }
+                        if (!skip)
+                            stream_row<32, CAP, PKV, ACC, VAL>(p, cur.b0, cur.b1, lane, cur.av, pkeys, acc, probe_arg,
+                                                               cnt);
+                    }
+                    tc = tn;
+                    tn = tnn;
                 }
-                stream_brow<32, VAL>(p, b0, b1, lane, [&](int x, uint32_t bv) {
-                    int s;
-                    if constexpr (KIND == K_MSA_BLOCK) {
-                        const int y = x - lo_col;
-                        s = (y >= 0 && y < WIN && ((bits[y >> 5] >> (y & 31)) & 1u)) ? y : -1;
-                    } else if constexpr (KIND == K_MCA_BLOCK) {
-                        s = sorted_find(keys, clen, x);
-                    } else {
-                        s = hash_find<CAP>(keys, x);
-                    }
-                    if (s >= 0) {
-                        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), av * bv);
-                        else cnt += av * bv;
-                    }
-                });
             }
         }
         __syncthreads();
@@ -499,23 +579,30 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
     void (*fn)(KArgs);
     int nt;
     if constexpr (X.kind == K_HASH_GROUP || X.kind == K_MCA_GROUP) {
-        constexpr int NTV = (V == 4) ? 128 : NT_GROUP;
+        constexpr int NTV = group_cta_threads(V);
         constexpr bool MCA = X.kind == K_MCA_GROUP;
         constexpr int CAPV = MCA ? X.chunk : X.cap;
-        fn = k_group<X.G, NTV, CAPV, X.chunk, MCA, EPI, VAL>;
+        fn = k_group<X.G, X.sub, NTV, CAPV, X.chunk, MCA, EPI, VAL>;
         nt = NTV;
     } else {
-        constexpr int CAPV = (X.kind == K_MSA_BLOCK) ? (W ? X.cap_write : X.cap) : (W ? X.cap_write : X.cap);
+        constexpr int CAPV = W ? X.cap_write : X.cap;
         constexpr int CHV = W ? X.chunk_write : X.chunk;
         fn = k_block<X.G, X.kind, CAPV, CHV, X.split_log2, EPI, VAL>;
         nt = X.G;
     }
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SMEM));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, SMEM);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
+    // resident CTAs per SM, computed once per kernel instance (and device)
+    static int per_sm_cache[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &per_sm = per_sm_cache[dev & 63];
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(SMEM));
+        if (e != cudaSuccess) return e;
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, nt, SMEM);
+        if (e != cudaSuccess) return e;
+        per_sm = n < 1 ? 1 : n;
+    }
     fn<<<num_sms * per_sm, nt, SMEM, s>>>(args);
     return cudaGetLastError();
 }
@@ -540,6 +627,9 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 7: return launch_variant_v<7>(a, epi, val, sms, s);
         case 8: return launch_variant_v<8>(a, epi, val, sms, s);
         case 9: return launch_variant_v<9>(a, epi, val, sms, s);
+        case 10: return launch_variant_v<10>(a, epi, val, sms, s);
+        case 11: return launch_variant_v<11>(a, epi, val, sms, s);
+        case 12: return launch_variant_v<12>(a, epi, val, sms, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -623,15 +713,29 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     args.row_key = rq.row_key;
     args.vec = (reinterpret_cast<uintptr_t>(B.col) % 16) == 0;
     const bool val = rq.use_values && (A.val || B.val);
+    // the variant kernels are independent: fork them onto side streams so
+    // that one variant's tail overlaps the others, then join (capturable)
+    SideStreams &side = side_streams();
+    const bool fork = rq.force_variant < 0;
+    if (fork) GK_CUDA(cudaEventRecord(side.fork, s));
     ProfWindow prof(s, NV);
     for (int v = 0; v < NV; ++v) {
         if (rq.force_variant >= 0 && v != rq.force_variant) continue;
         args.v = v;
-        prof.begin(v);
-        cudaError_t e = launch_variant(v, args, rq.epi, val, sms, s);
+        cudaStream_t vs = s;
+        if (fork) {
+            vs = side.s[v];
+            GK_CUDA(cudaStreamWaitEvent(vs, side.fork, 0));
+        }
+        prof.begin(v, vs);
+        cudaError_t e = launch_variant(v, args, rq.epi, val, sms, vs);
         if (e != cudaSuccess) return cuda_fail(e, "masked SpGEMM variant launch");
-        prof.end(v);
+        prof.end(v, vs);
         note_launches(1);
+        if (fork) {
+            GK_CUDA(cudaEventRecord(side.join[v], vs));
+            GK_CUDA(cudaStreamWaitEvent(s, side.join[v], 0));
+        }
     }
     if (prof.active()) {
         // attribute the bins' work to the variants that ran them

@@ -1,0 +1,300 @@
+// graphkokkos.hpp — header-only C++ drop-in for GraphKokkos' hot path.
+//
+// Provides the reference's type and function names with the reference's
+// signatures, implemented on top of the C ABI in gk_b200.h (libgk_b200.so):
+//
+//   spMtx<T>            include/matrix.h:33-175 (m, n, nz, Rst, Col, Val; shallow
+//                       reference-counted copies, deep_copy explicit)
+//   denseMtx<T>         include/matrix.h:548-630 (row-major Val(i*n+j))
+//   mxmOp<T>            src/main.cpp:13-14
+//   mxmm_msa / mxmm_mca / mxmm_naive / mxmm_gpu
+//                       include/matrix_la.h:478-694, :936-1068 — C<M> = A·B, C
+//                       resized to M's pattern with explicit zeros kept (:564-568)
+//   triangle_counting_masked_sandia   src/main.cpp:69-90
+//   k_truss                           src/main.cpp:94-141
+//   betweenness_centrality_batch      include/betweenness_centrality.h:406-506
+//   transpose / extract_lower_triangle / build_symm_from_lower /
+//   build_adjacency_matrix            include/matrix_la.h:155-179, include/matrix.h:643-726
+//
+// Differences from the reference, all deliberate:
+//   * storage is host memory owned by std::shared_ptr (no Kokkos); Rst is
+//     int64 so graphs beyond 2^31 entries fit;
+//   * every operation runs on the GPU through libgk_b200.so; `isParallel` is
+//     accepted and ignored;
+//   * errors throw std::runtime_error carrying gk_last_error_string() (the
+//     reference throws const char* / int);
+//   * betweenness_centrality_batch(isParallel, A, b) keeps the reference's
+//     float return type and sources 0..b-1 but computes in FP64; the overload
+//     taking a source list returns the FP64 scores.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../gk_b200.h"
+
+namespace gkb_detail {
+
+inline void check(int status) {
+    if (status != GK_OK) throw std::runtime_error(std::string("gk_b200: ") + gk_last_error_string());
+}
+
+// Minimal shared 1-D array with the View call syntax used by the reference
+// (operator() and operator[] returning T&, data(), size()).
+template <typename T>
+class Array {
+public:
+    Array() = default;
+    explicit Array(size_t n) : p_(std::make_shared<std::vector<T>>(n)) {}
+    T &operator()(size_t i) const { return (*p_)[i]; }
+    T &operator[](size_t i) const { return (*p_)[i]; }
+    T *data() const { return p_ ? p_->data() : nullptr; }
+    size_t size() const { return p_ ? p_->size() : 0; }
+    void resize(size_t n) {
+        if (!p_) p_ = std::make_shared<std::vector<T>>(n);
+        else if (p_->size() != n) {
+            auto q = std::make_shared<std::vector<T>>(n);
+            std::copy(p_->begin(), p_->begin() + std::min(n, p_->size()), q->begin());
+            p_ = q;
+        }
+    }
+    Array clone() const {
+        Array a(size());
+        if (size()) std::copy(p_->begin(), p_->end(), a.p_->begin());
+        return a;
+    }
+
+private:
+    std::shared_ptr<std::vector<T>> p_;
+};
+
+}  // namespace gkb_detail
+
+template <typename ValT>
+class spMtx {
+public:
+    size_t m = 0, n = 0, nz = 0;
+    gkb_detail::Array<int64_t> Rst;
+    gkb_detail::Array<int> Col;
+    gkb_detail::Array<ValT> Val;
+
+    spMtx() = default;
+    spMtx(size_t m_, size_t n_) : m(m_), n(n_), Rst(m_ + 1) {}
+    spMtx(size_t m_, size_t n_, size_t nz_) : m(m_), n(n_), nz(nz_), Rst(m_ + 1), Col(nz_), Val(nz_) {}
+
+    void resizeRows(size_t newM) {
+        m = newM;
+        Rst.resize(newM + 1);
+    }
+    void resizeVals(size_t newNz) {
+        Col.resize(newNz);
+        Val.resize(newNz);
+        nz = newNz;
+    }
+    void deep_copy(const spMtx &src) {
+        m = src.m;
+        n = src.n;
+        nz = src.nz;
+        Rst = src.Rst.clone();
+        Col = src.Col.clone();
+        Val = src.Val.clone();
+    }
+    spMtx extractRows(size_t begin, size_t end) const {
+        spMtx r(end - begin, n, static_cast<size_t>(Rst[end] - Rst[begin]));
+        for (size_t i = 0; i <= end - begin; ++i) r.Rst(i) = Rst(i + begin) - Rst(begin);
+        for (size_t j = 0; j < r.nz; ++j) {
+            r.Col(j) = Col(Rst(begin) + j);
+            r.Val(j) = Val(Rst(begin) + j);
+        }
+        return r;
+    }
+    bool operator==(const spMtx &o) const {
+        if (m != o.m || n != o.n || nz != o.nz) return false;
+        for (size_t i = 0; i <= m; ++i)
+            if (Rst(i) != o.Rst(i)) return false;
+        for (size_t j = 0; j < nz; ++j)
+            if (Col(j) != o.Col(j) || Val(j) != o.Val(j)) return false;
+        return true;
+    }
+    // view of this matrix for the C ABI (values as given, or pattern-only)
+    gk_csr csr(bool with_values = true) const {
+        static_assert(std::is_same<ValT, int>::value, "the GPU operators take int matrices (spMtx<int>)");
+        return gk_csr{static_cast<int64_t>(m), static_cast<int64_t>(n), static_cast<int64_t>(nz), Rst.data(),
+                      Col.data(), with_values ? Val.data() : nullptr};
+    }
+};
+
+template <typename ValT>
+void deep_copy(spMtx<ValT> &dst, const spMtx<ValT> &src) {
+    dst.deep_copy(src);
+}
+
+template <typename ValT>
+class denseMtx {
+public:
+    size_t m = 0, n = 0;
+    gkb_detail::Array<ValT> Val;
+    denseMtx() = default;
+    denseMtx(size_t m_, size_t n_) : m(m_), n(n_), Val(m_ * n_) {}
+    template <typename V2>
+    denseMtx(const spMtx<V2> &s) : m(s.m), n(s.n), Val(s.m * s.n) {
+        for (size_t i = 0; i < s.m; ++i)
+            for (int64_t k = s.Rst(i); k < s.Rst(i + 1); ++k) Val(i * n + s.Col(k)) = static_cast<ValT>(s.Val(k));
+    }
+};
+
+template <typename T>
+using mxmOp = void (*)(bool, const spMtx<T> &, const spMtx<T> &, const spMtx<T> &, spMtx<T> &);
+
+namespace gkb_detail {
+template <typename T, typename U>
+void mxmm_with(int accum, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &M, spMtx<T> &C) {
+    static_assert(std::is_same<T, int>::value, "the GPU operators take int matrices (spMtx<int>)");
+    // C takes M's pattern, explicit zeros kept (include/matrix_la.h:564-568)
+    spMtx<T> R(M.m, M.n, M.nz);
+    std::copy(M.Rst.data(), M.Rst.data() + M.m + 1, R.Rst.data());
+    if (M.nz) std::copy(M.Col.data(), M.Col.data() + M.nz, R.Col.data());
+    gk_csr a = A.csr(), b = B.csr();
+    gk_csr mm{static_cast<int64_t>(M.m), static_cast<int64_t>(M.n), static_cast<int64_t>(M.nz), M.Rst.data(),
+              M.Col.data(), nullptr};
+    check(gk_mxmm_masked(&a, &b, &mm, R.Val.data(), GK_PLUS_TIMES, GK_SCHED_PLAIN, accum, nullptr));
+    C = R;
+}
+}  // namespace gkb_detail
+
+// mxmOp family (include/matrix_la.h:87-149).  All run on the GPU; the name
+// selects the accumulator family the scheduler is restricted to.
+template <typename T, typename U>
+void mxmm_msa(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &M, spMtx<T> &C) {
+    gkb_detail::mxmm_with(GK_ACCUM_MSA, A, B, M, C);
+}
+template <typename T, typename U>
+void mxmm_mca(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &M, spMtx<T> &C) {
+    gkb_detail::mxmm_with(GK_ACCUM_MCA, A, B, M, C);
+}
+template <typename T>
+void mxmm_naive(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, spMtx<T> &C) {
+    gkb_detail::mxmm_with(GK_ACCUM_HASH, A, B, M, C);
+}
+// Scheduler's choice per row bin (plain heuristic).
+template <typename T>
+void mxmm_gpu(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, spMtx<T> &C) {
+    gkb_detail::mxmm_with(GK_ACCUM_AUTO, A, B, M, C);
+}
+
+// ----- CSR transforms ------------------------------------------------------------
+template <typename T>
+spMtx<T> transpose(const spMtx<T> &A) {
+    spMtx<T> R(A.n, A.m, A.nz);
+    gk_csr a = A.csr();
+    gkb_detail::check(gk_transpose(&a, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
+    return R;
+}
+
+template <typename T>
+spMtx<T> extract_lower_triangle(const spMtx<T> &A) {
+    spMtx<T> R(A.m, A.n, A.nz);
+    gk_csr a = A.csr(false);
+    int64_t nz = 0;
+    gkb_detail::check(gk_extract_lower(&a, R.Rst.data(), R.Col.data(), &nz, nullptr));
+    // values follow their columns: the lower part of each row is its prefix
+    for (size_t i = 0; i < A.m; ++i)
+        for (int64_t j = 0; j < R.Rst(i + 1) - R.Rst(i); ++j) R.Val(R.Rst(i) + j) = A.Val(A.Rst(i) + j);
+    R.resizeVals(static_cast<size_t>(nz));
+    return R;
+}
+
+template <typename T>
+spMtx<T> build_symm_from_lower(const spMtx<T> &Low) {
+    spMtx<T> U = transpose(Low);
+    spMtx<T> R(Low.m, Low.n, 2 * Low.nz);
+    size_t jr = 0;
+    for (size_t i = 0; i < Low.m; ++i) {
+        int64_t jl = Low.Rst(i), xl = Low.Rst(i + 1), ju = U.Rst(i), xu = U.Rst(i + 1);
+        while (jl < xl && ju < xu) {
+            if (Low.Col(jl) < U.Col(ju)) { R.Col(jr) = Low.Col(jl); R.Val(jr++) = Low.Val(jl++); }
+            else { R.Col(jr) = U.Col(ju); R.Val(jr++) = U.Val(ju++); }
+        }
+        while (jl < xl) { R.Col(jr) = Low.Col(jl); R.Val(jr++) = Low.Val(jl++); }
+        while (ju < xu) { R.Col(jr) = U.Col(ju); R.Val(jr++) = U.Val(ju++); }
+        R.Rst(i + 1) = static_cast<int64_t>(jr);
+    }
+    return R;
+}
+
+template <typename T>
+spMtx<int> build_adjacency_matrix(const spMtx<T> &G) {
+    spMtx<int> R(G.m, G.n, G.nz);
+    std::copy(G.Rst.data(), G.Rst.data() + G.m + 1, R.Rst.data());
+    for (size_t j = 0; j < G.nz; ++j) {
+        R.Col(j) = G.Col(j);
+        R.Val(j) = 1;
+    }
+    return R;
+}
+
+// ----- algorithms --------------------------------------------------------------------
+// Triangle count (src/main.cpp:69-90).  With one of this header's operators
+// the count runs fused on the GPU (no C materialised); any other mxmOp is
+// called as the reference does and C summed on the host.
+inline int64_t triangle_counting_masked_sandia(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel) {
+    spMtx<int> L = extract_lower_triangle(A);
+    const bool ours = matrixMult == static_cast<mxmOp<int>>(mxmm_msa<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_mca<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_naive<int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_gpu<int>);
+    if (ours) {
+        gk_csr l = L.csr(false);
+        uint64_t count = 0;
+        gkb_detail::check(gk_tc_count(&l, &count, GK_SCHED_PLAIN, nullptr));
+        return static_cast<int64_t>(count);
+    }
+    spMtx<int> C;
+    matrixMult(isParallel, L, L, L, C);
+    int64_t sum = 0;
+    for (size_t j = 0; j < C.nz; ++j) sum += C.Val(j);
+    return sum;
+}
+
+// k-truss (src/main.cpp:94-141).  matrixMult is accepted for signature
+// compatibility; the support products run on the GPU engine.
+inline spMtx<int> k_truss(const spMtx<int> &A, int k, mxmOp<int>, bool, int *iterations = nullptr) {
+    spMtx<int> C(A.m, A.n, A.nz);
+    std::copy(A.Rst.data(), A.Rst.data() + A.m + 1, C.Rst.data());
+    if (A.nz) std::copy(A.Col.data(), A.Col.data() + A.nz, C.Col.data());
+    gk_csr_mut io{static_cast<int64_t>(A.m), static_cast<int64_t>(A.n), static_cast<int64_t>(A.nz), C.Rst.data(),
+                  C.Col.data()};
+    int iters = 0;
+    gkb_detail::check(gk_ktruss(&io, k, &iters, GK_SCHED_PLAIN, nullptr));
+    C.resizeVals(static_cast<size_t>(io.nnz));
+    for (size_t j = 0; j < C.nz; ++j) C.Val(j) = 1;
+    if (iterations) *iterations = iters;
+    return C;
+}
+
+// Batched BC with sources 0..min(n, batchSize)-1, as the reference
+// (include/betweenness_centrality.h:406-447); computed in FP64.
+inline std::vector<float> betweenness_centrality_batch(bool, const spMtx<int> &A, size_t batchSize) {
+    if (A.m != A.n) throw "non-square matrix; BC is only for square matrices";
+    const size_t b = std::min(A.n, batchSize);
+    std::vector<int32_t> src(b);
+    for (size_t j = 0; j < b; ++j) src[j] = static_cast<int32_t>(j);
+    std::vector<double> d(A.m);
+    gk_csr a = A.csr();
+    gkb_detail::check(gk_bc_batch(&a, src.data(), static_cast<int>(b), d.data(), GK_SCHED_PLAIN, nullptr));
+    return std::vector<float>(d.begin(), d.end());
+}
+
+inline std::vector<double> betweenness_centrality_batch(const spMtx<int> &A, const std::vector<int32_t> &sources) {
+    std::vector<double> d(A.m);
+    gk_csr a = A.csr();
+    gkb_detail::check(gk_bc_batch(&a, sources.data(), static_cast<int>(sources.size()), d.data(), GK_SCHED_PLAIN,
+                                  nullptr));
+    return d;
+}
