@@ -33,6 +33,13 @@ __device__ __forceinline__ int hash_slot(int x) {
     return static_cast<int>((static_cast<uint32_t>(x) * 0x9E3779B1u) >> (32 - LOG2));
 }
 
+// Bit of x in a 2^FLOG-bit filter (a second multiplicative hash, independent
+// of the table slot's).
+template <int FLOG>
+__device__ __forceinline__ uint32_t filter_bit(int x) {
+    return (static_cast<uint32_t>(x) * 0x85EBCA77u) >> (32 - FLOG);
+}
+
 // Inserts x into an open-addressing (linear probing) table; concurrent
 // inserts of distinct keys are safe.  The caller guarantees fewer than CAP
 // keys, so a free slot always exists; the probe count is bounded anyway.

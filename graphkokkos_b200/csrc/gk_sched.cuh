@@ -41,35 +41,38 @@ struct Variant {
     int chunk;      // mask entries per item (HASH/MCA); unused by MSA
     int chunk_write;
     int split_log2; // block kinds: work per item before a row's A entries are split
+    int flog;       // block HASH kinds: log2 bits of the bitmap filter in front of the table
+    int batch;      // items a CTA (group kinds: a warp) takes per fetch
     int accum;      // gk_accum family this variant belongs to
 };
 
 constexpr int NV = 13;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
-// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, accum family
+// Hash tables run at load factor <= 1/4 (chunk <= cap/4) except variant 10.
+// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum
 #define GK_VARIANT_TABLE { \
-    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0, 3},   \
-    {K_HASH_GROUP,   8,  4,   128,   128,    32,    32,   0, 3},   \
-    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0, 3},   \
-    {K_HASH_GROUP,  16,  4,   256,   256,    64,    64,   0, 3},   \
-    {K_HASH_GROUP,  16, 16,   256,   256,    64,    64,   0, 3},   \
-    {K_HASH_GROUP,  32,  8,   512,   512,   128,   128,   0, 3},   \
-    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 3},   \
-    {K_HASH_GROUP,  32, 16,  2048,  2048,   512,   512,   0, 3},   \
-    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  18, 3},   \
-    {K_HASH_BLOCK, 512, 32, 32768, 16384, 16384,  8192,  20, 3},   \
-    {K_MCA_GROUP,   32,  8,   256,   256,   256,   256,   0, 2},   \
-    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20, 2},   \
-    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20, 1},   \
+    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3},   \
+    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3},   \
+    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 11, 1, 3},   \
+    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 11, 8, 3},   \
+    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 12, 4, 3},   \
+    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 12, 4, 3},   \
+    {K_HASH_BLOCK, 128, 32,  4096,  4096,  1024,  1024,  18, 14, 2, 3},   \
+    {K_HASH_BLOCK, 256, 32, 16384, 16384,  4096,  4096,  19, 16, 1, 3},   \
+    {K_HASH_BLOCK, 512, 32, 32768, 16384,  8192,  4096,  20, 17, 1, 3},   \
+    {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2},   \
+    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2},   \
+    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3},   \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
 __constant__ const Variant c_variants[NV] = GK_VARIANT_TABLE;  // runtime-indexed copy for device code
 #endif
-constexpr int NT_GROUP = 256;  // CTA size of the group kinds (variant 7 uses 128)
-__host__ __device__ constexpr int group_cta_threads(int v) { return v == 7 ? 128 : NT_GROUP; }
+constexpr int NT_GROUP = 256;  // CTA size of the group kinds
+__host__ __device__ constexpr int group_cta_threads(int) { return NT_GROUP; }
 // variant ids the heuristics name
-constexpr int V_MCA_GROUP = 10, V_MCA_BLOCK = 11, V_MSA_BLOCK = 12;
+constexpr int V_MCA_GROUP = 9, V_MCA_BLOCK = 10, V_MSA_BLOCK = 11;
 
 // ---- features of a bin (inputs of the learned scheduler) ---------------------
 constexpr int NFEAT = 8;

@@ -46,15 +46,15 @@ __host__ __device__ inline void bin_features(const BinStats &b, int epi, bool va
 __host__ __device__ inline int plain_variant(int bin, const BinStats &b) {
     const int qm = bin / NB_B, qb = bin % NB_B;  // log2 mask-row length, log2 mean B-row length
     int v;
-    if (qm <= 3) v = qb <= 3 ? 0 : (qb <= 6 ? 3 : 5);       // < 16 mask entries
-    else if (qm == 4) v = qb <= 4 ? 1 : (qb <= 6 ? 3 : 5);  // < 32
-    else if (qm == 5) v = qb <= 6 ? 3 : 5;                  // < 64
-    else if (qm == 6) v = qb <= 8 ? 5 : 6;                  // < 128
-    else if (qm <= 8) v = 7;                                // < 512
-    else if (qm <= 11) v = 8;                               // < 4096
-    else v = 9;
+    if (qm <= 3) v = qb <= 4 ? 0 : 3;       // < 16 mask entries: 4 threads, or a 2-warp CTA for long B rows
+    else if (qm == 4) v = qb <= 3 ? 1 : 3;  // < 32
+    else if (qm <= 6) v = qb <= 3 ? 2 : 3;  // < 128
+    else if (qm == 7) v = qb <= 5 ? 5 : 4;  // < 256: half-warps stream short B rows
+    else if (qm <= 9) v = 6;                // < 1024
+    else if (qm <= 11) v = 7;               // < 4096
+    else v = 8;
     const double mean_w = static_cast<double>(b.sum_work) / static_cast<double>(b.rows ? b.rows : 1);
-    if (v <= 7 && mean_w > double(1 << 21)) v = 8;  // heavy rows: split over CTAs
+    if (v <= 2 && mean_w > double(1 << 16)) v = 3;  // heavy rows: CTA kinds split them
     return v;
 }
 

@@ -42,6 +42,7 @@ struct KArgs {
     DevCsr A, B, M;
     const int32_t *rowlist;  // rows sorted by variant
     const int *voff;         // [NV+1] offsets into rowlist
+    const int *vsimple;      // [NV] rows of each variant that are a single item (listed first)
     const int64_t *item_ex;  // exclusive prefix of items per rowlist entry (block kinds)
     const int64_t *work;     // per-row work
     unsigned int *fetch;     // [NV] dynamic item counters (block kinds)
@@ -134,29 +135,49 @@ __device__ __forceinline__ int64_t items_of_row(int v, bool write, int64_t mlen,
     return nch * num_splits(w, alen, V.split_log2);
 }
 
-// Counting sort of the rows by variant, one CTA-level reservation per variant.
-__global__ void k_count_rows(int64_t m, const uint16_t *bin, const int *var_of_bin, int force_variant,
-                             int *vcount) {
-    __shared__ int s_cnt[NV];
-    if (threadIdx.x < NV) s_cnt[threadIdx.x] = 0;
-    __syncthreads();
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += stride) {
-        const uint16_t b = bin[r];
-        if (b == BIN_SKIP) continue;
-        const int v = force_variant >= 0 ? force_variant : var_of_bin[b];
-        atomicAdd(&s_cnt[v], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < NV && s_cnt[threadIdx.x]) atomicAdd(&vcount[threadIdx.x], s_cnt[threadIdx.x]);
+// Variant and item count of row r (-1 when the row has no work).
+__device__ __forceinline__ int row_variant(int64_t r, const uint16_t *bin, const int *var_of_bin, int force_variant) {
+    const uint16_t b = bin[r];
+    if (b == BIN_SKIP) return -1;
+    return force_variant >= 0 ? force_variant : var_of_bin[b];
 }
 
-__global__ void k_offsets(const int *vcount, int *voff, int *vcursor, unsigned int *fetch) {
+__device__ __forceinline__ int64_t row_items(const DevCsr &A, const DevCsr &M, const int64_t *work, int64_t r, int v,
+                                             bool write) {
+    const int64_t m0 = M.rp[r], mlen = M.rp[r + 1] - m0;
+    return items_of_row(v, write, mlen, A.rp[r + 1] - A.rp[r], work[r], M.col + m0);
+}
+
+// Counting sort of the rows by variant.  Within a variant's segment the rows
+// that are a single item come first, so the kernels map those items to rows
+// without a search; rows split into several items follow.
+__global__ void k_count_rows(DevCsr A, DevCsr M, const int64_t *work, const uint16_t *bin, const int *var_of_bin,
+                             int force_variant, bool write, int *vcount, int *vsimple) {
+    __shared__ int s_cnt[NV], s_simple[NV];
+    if (threadIdx.x < NV) s_cnt[threadIdx.x] = s_simple[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.m; r += stride) {
+        const int v = row_variant(r, bin, var_of_bin, force_variant);
+        if (v < 0) continue;
+        atomicAdd(&s_cnt[v], 1);
+        if (row_items(A, M, work, r, v, write) == 1) atomicAdd(&s_simple[v], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < NV && s_cnt[threadIdx.x]) {
+        atomicAdd(&vcount[threadIdx.x], s_cnt[threadIdx.x]);
+        atomicAdd(&vsimple[threadIdx.x], s_simple[threadIdx.x]);
+    }
+}
+
+// vcursor[2v]: next single-item slot of variant v, vcursor[2v+1]: next multi-item slot.
+__global__ void k_offsets(const int *vcount, const int *vsimple, int *voff, int *vcursor, unsigned int *fetch) {
     if (threadIdx.x == 0) {
         int acc = 0;
         for (int v = 0; v < NV; ++v) {
             voff[v] = acc;
-            vcursor[v] = acc;
+            vcursor[2 * v] = acc;
+            vcursor[2 * v + 1] = acc + vsimple[v];
             fetch[v] = 0;
             acc += vcount[v];
         }
@@ -167,28 +188,30 @@ __global__ void k_offsets(const int *vcount, int *voff, int *vcursor, unsigned i
 __global__ void k_scatter_rows(DevCsr A, DevCsr M, const int64_t *work, const uint16_t *bin,
                                const int *var_of_bin, int force_variant, bool write, int *vcursor,
                                int32_t *rowlist, int64_t *item_n) {
-    __shared__ int s_cnt[NV], s_base[NV];
+    __shared__ int s_cnt[2 * NV], s_base[2 * NV];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < A.m; base += stride) {
-        if (threadIdx.x < NV) s_cnt[threadIdx.x] = 0;
+        if (threadIdx.x < 2 * NV) s_cnt[threadIdx.x] = 0;
         __syncthreads();
         const int64_t r = base + threadIdx.x;
-        int v = -1, local = 0;
+        int slot = -1, local = 0;
+        int64_t items = 0;
         if (r < A.m) {
-            const uint16_t b = bin[r];
-            if (b != BIN_SKIP) {
-                v = force_variant >= 0 ? force_variant : var_of_bin[b];
-                local = atomicAdd(&s_cnt[v], 1);
+            const int v = row_variant(r, bin, var_of_bin, force_variant);
+            if (v >= 0) {
+                items = row_items(A, M, work, r, v, write);
+                slot = 2 * v + (items == 1 ? 0 : 1);
+                local = atomicAdd(&s_cnt[slot], 1);
             }
         }
         __syncthreads();
-        if (threadIdx.x < NV && s_cnt[threadIdx.x]) s_base[threadIdx.x] = atomicAdd(&vcursor[threadIdx.x], s_cnt[threadIdx.x]);
+        if (threadIdx.x < 2 * NV && s_cnt[threadIdx.x])
+            s_base[threadIdx.x] = atomicAdd(&vcursor[threadIdx.x], s_cnt[threadIdx.x]);
         __syncthreads();
-        if (v >= 0) {
-            const int pos = s_base[v] + local;
+        if (slot >= 0) {
+            const int pos = s_base[slot] + local;
             rowlist[pos] = static_cast<int32_t>(r);
-            const int64_t m0 = M.rp[r], mlen = M.rp[r + 1] - m0;
-            item_n[pos] = items_of_row(v, write, mlen, A.rp[r + 1] - A.rp[r], work[r], M.col + m0);
+            item_n[pos] = items;
         }
         __syncthreads();
     }
@@ -204,9 +227,15 @@ enum : int { PK_HASH = 0, PK_MCA = 1, PK_MSA = 2 };
 // HASH  slot of x in a CAP-slot hash set;  MCA  position of x in the sorted
 // chunk keys[0, clen);  MSA  x - base if its bit is set in a 2^CAP-column
 // window bitmap (keys reinterpreted as words).
-template <int CAP, int PK, bool ACC>
-__device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, int *acc, int clen, unsigned &cnt) {
+template <int CAP, int PK, bool ACC, int FLOG = 0>
+__device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, int *acc, int clen, unsigned &cnt,
+                                           const unsigned *filt = nullptr) {
     int s;
+    if constexpr (PK == PK_HASH && FLOG > 0) {
+        // bitmap filter first: most B elements are not mask columns
+        const uint32_t h = filter_bit<FLOG>(x);
+        if (!((filt[h >> 5] >> (h & 31)) & 1u)) return;
+    }
     if constexpr (PK == PK_MSA) {
         const int y = x - clen;  // clen carries the window base for MSA
         s = (y >= 0 && y < (1 << CAP) && ((reinterpret_cast<const unsigned *>(keys)[y >> 5] >> (y & 31)) & 1u)) ? y : -1;
@@ -221,46 +250,106 @@ __device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, i
     }
 }
 
+// Filter bit of x (0/1) and the exact test of a filter candidate.
+template <int FLOG>
+__device__ __forceinline__ uint32_t cand_bit(int x, const unsigned *filt) {
+    const uint32_t h = filter_bit<FLOG>(x);
+    return (filt[h >> 5] >> (h & 31)) & 1u;
+}
+
+template <int CAP, bool ACC>
+__device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, int *acc, unsigned &cnt) {
+    const int s = hash_find<CAP>(keys, x);
+    if (s >= 0) {
+        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), w);
+        else cnt += w;
+    }
+}
+
 // The SUB lanes of a sub-group stream B[b0, b1): 16-byte vector loads, two in
 // flight per lane, scalar head/tail; with values, scalar loads of col and val.
-template <int SUB, int CAP, int PK, bool ACC, bool VAL>
+// With a filter, the eight elements of two vectors are tested against the
+// filter without branches and only the candidates take the exact lookup.
+template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0>
 __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b1, int sl, uint32_t av,
-                                           const int *keys, int *acc, int clen, unsigned &cnt) {
+                                           const int *keys, int *acc, int clen, unsigned &cnt,
+                                           const unsigned *filt = nullptr) {
     const int32_t *__restrict__ bc = p.B.col;
+    if constexpr (PK == PK_HASH && FLOG > 0 && !VAL) {
+        if (p.vec) {
+            int64_t h1 = (b0 + 3) & ~int64_t(3);
+            if (h1 > b1) h1 = b1;
+            if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
+            const int4 *__restrict__ base = reinterpret_cast<const int4 *>(bc) + (h1 >> 2);
+            const int n4 = static_cast<int>((b1 >> 2) - (h1 >> 2));
+            int q = sl;
+            for (; q + SUB < n4; q += 2 * SUB) {
+                const int4 x = __ldg(base + q);
+                const int4 y = __ldg(base + q + SUB);
+                const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
+                                   (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3) |
+                                   (cand_bit<FLOG>(y.x, filt) << 4) | (cand_bit<FLOG>(y.y, filt) << 5) |
+                                   (cand_bit<FLOG>(y.z, filt) << 6) | (cand_bit<FLOG>(y.w, filt) << 7);
+                if (m) {
+                    if (m & 1u) exact_hash<CAP, ACC>(x.x, av, keys, acc, cnt);
+                    if (m & 2u) exact_hash<CAP, ACC>(x.y, av, keys, acc, cnt);
+                    if (m & 4u) exact_hash<CAP, ACC>(x.z, av, keys, acc, cnt);
+                    if (m & 8u) exact_hash<CAP, ACC>(x.w, av, keys, acc, cnt);
+                    if (m & 16u) exact_hash<CAP, ACC>(y.x, av, keys, acc, cnt);
+                    if (m & 32u) exact_hash<CAP, ACC>(y.y, av, keys, acc, cnt);
+                    if (m & 64u) exact_hash<CAP, ACC>(y.z, av, keys, acc, cnt);
+                    if (m & 128u) exact_hash<CAP, ACC>(y.w, av, keys, acc, cnt);
+                }
+            }
+            if (q < n4) {
+                const int4 x = __ldg(base + q);
+                const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
+                                   (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3);
+                if (m & 1u) exact_hash<CAP, ACC>(x.x, av, keys, acc, cnt);
+                if (m & 2u) exact_hash<CAP, ACC>(x.y, av, keys, acc, cnt);
+                if (m & 4u) exact_hash<CAP, ACC>(x.z, av, keys, acc, cnt);
+                if (m & 8u) exact_hash<CAP, ACC>(x.w, av, keys, acc, cnt);
+            }
+            int64_t tl = (b1 >> 2) << 2;
+            if (tl < h1) tl = h1;
+            if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
+            return;
+        }
+    }
     if (!VAL && p.vec) {
         int64_t h1 = (b0 + 3) & ~int64_t(3);
         if (h1 > b1) h1 = b1;
-        if (b0 + sl < h1) probe_elem<CAP, PK, ACC>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt);
+        if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
         const int64_t v1 = b1 >> 2;
         const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
         int64_t q = (h1 >> 2) + sl;
         for (; q + SUB < v1; q += 2 * SUB) {
             const int4 x = __ldg(bv + q);
             const int4 y = __ldg(bv + q + SUB);
-            probe_elem<CAP, PK, ACC>(x.x, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.y, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.z, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.w, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(y.x, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(y.y, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(y.z, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(y.w, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.w, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(y.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(y.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(y.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(y.w, av, keys, acc, clen, cnt, filt);
         }
         if (q < v1) {
             const int4 x = __ldg(bv + q);
-            probe_elem<CAP, PK, ACC>(x.x, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.y, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.z, av, keys, acc, clen, cnt);
-            probe_elem<CAP, PK, ACC>(x.w, av, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x.w, av, keys, acc, clen, cnt, filt);
         }
         int64_t tl = v1 << 2;
         if (tl < h1) tl = h1;
-        if (tl + sl < b1) probe_elem<CAP, PK, ACC>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt);
+        if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
     } else {
         const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
         for (int64_t j = b0 + sl; j < b1; j += SUB) {
             const uint32_t w = (VAL && bvals) ? av * static_cast<uint32_t>(__ldg(bvals + j)) : av;
-            probe_elem<CAP, PK, ACC>(__ldg(bc + j), w, keys, acc, clen, cnt);
+            probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + j), w, keys, acc, clen, cnt, filt);
         }
     }
 }
@@ -283,10 +372,10 @@ __device__ __forceinline__ BRow brow_of(const KArgs &p, int k, int64_t t) {
 // Streams the B rows of A entries t = first, first+step, ... < a1 with one
 // sub-group of SUB lanes: the next entry's row bounds and the entry after
 // that's column are loaded while the current row streams.
-template <int SUB, int CAP, int PK, bool ACC, bool VAL>
+template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG>
 __device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, int64_t a1, int step, int sl,
                                                bool chunked, int lo_col, int hi_col, const int *keys, int *acc,
-                                               int clen, unsigned &cnt) {
+                                               int clen, unsigned &cnt, const unsigned *filt) {
     const unsigned smask = group_mask<SUB>();
     int64_t t = first;
     if (t >= a1) return;
@@ -307,31 +396,39 @@ __device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, in
                     cur.b0 = lo;
                 }
             }
-            if (!skip) stream_row<SUB, CAP, PK, ACC, VAL>(p, cur.b0, cur.b1, sl, cur.av, keys, acc, clen, cnt);
+            if (!skip)
+                stream_row<SUB, CAP, PK, ACC, VAL, FLOG>(p, cur.b0, cur.b1, sl, cur.av, keys, acc, clen, cnt, filt);
         }
         t = tn;
     }
 }
 
 // G threads per row; the row's A entries are dealt round-robin to G/SUB
-// sub-groups of SUB lanes that stream their B rows concurrently.
-template <int G, int SUB, int NT, int CAP, int CHUNK, bool MCA, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT) k_group(KArgs p) {
+// sub-groups of SUB lanes that stream their B rows concurrently.  Each group
+// takes its next row from a global counter, so groups never wait on each
+// other for work.
+template <int G, int SUB, int NT, int CAP, int CHUNK, bool MCA, int FLOG, int EPI, bool VAL>
+__global__ void __launch_bounds__(NT, 1536 / NT) k_group(KArgs p) {
     constexpr int NG = NT / G;
     constexpr int S = G / SUB;
     constexpr bool ACC = (EPI == EPI_WRITE);
+    constexpr int FW = (!MCA && FLOG > 0) ? (1 << FLOG) / 32 : 0;  // filter words per group
     extern __shared__ int smem[];
-    __shared__ unsigned long long s_red[NT / 32];
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
     const int sg = lane / SUB, sl = lane % SUB;
     int *keys = smem + g * CAP;
     int *acc = smem + NG * CAP + g * CAP;
+    unsigned *filt = reinterpret_cast<unsigned *>(smem + NG * CAP * (ACC ? 2 : 1)) + g * FW;
     const unsigned gmask = group_mask<G>();
     const int begin = p.voff[p.v], end = p.voff[p.v + 1];
     unsigned long long local = 0;
 
-    for (int idx = begin + blockIdx.x * NG + g; idx < end; idx += gridDim.x * NG) {
+    while (true) {
+        int got = 0;
+        if (lane == 0) got = static_cast<int>(atomicAdd(p.fetch + p.v, 1u));
+        const int idx = begin + __shfl_sync(gmask, got, 0, G);
+        if (idx >= end) break;
         const int row = p.rowlist[idx];
         const int64_t m0 = p.M.rp[row];
         const int mlen = static_cast<int>(p.M.rp[row + 1] - m0);
@@ -352,14 +449,22 @@ __global__ void __launch_bounds__(NT) k_group(KArgs p) {
                     keys[s] = EMPTY_KEY;
                     if (ACC) acc[s] = 0;
                 }
+                for (int wd = lane; wd < FW; wd += G) filt[wd] = 0u;
                 __syncwarp(gmask);
-                for (int q = c0 + lane; q < c1; q += G) hash_insert<CAP>(keys, mc[q]);
+                for (int q = c0 + lane; q < c1; q += G) {
+                    const int x = mc[q];
+                    hash_insert<CAP>(keys, x);
+                    if constexpr (FW > 0) {
+                        const uint32_t h = filter_bit<FLOG>(x);
+                        atomicOr(filt + (h >> 5), 1u << (h & 31));
+                    }
+                }
             }
             __syncwarp(gmask);
             const int lo_col = mc[c0], hi_col = mc[c1 - 1];
             unsigned cnt = 0;
-            stream_entries<SUB, CAP, MCA ? PK_MCA : PK_HASH, ACC, VAL>(p, a0 + sg, a1, S, sl, chunked, lo_col,
-                                                                       hi_col, keys, acc, clen, cnt);
+            stream_entries<SUB, CAP, MCA ? PK_MCA : PK_HASH, ACC, VAL, (FW > 0 ? FLOG : 0)>(
+                p, a0 + sg, a1, S, sl, chunked, lo_col, hi_col, keys, acc, clen, cnt, filt);
             if (ACC) {
                 __syncwarp(gmask);
                 for (int q = c0 + lane; q < c1; q += G) {
@@ -378,178 +483,13 @@ __global__ void __launch_bounds__(NT) k_group(KArgs p) {
         }
     }
     if (EPI == EPI_SUM) {
-        const unsigned long long tot = block_sum(local, s_red);
-        if (threadIdx.x == 0 && tot) atomicAdd(p.sums, tot);
+        // groups leave at different times: reduce per group, no CTA barrier
+        const unsigned long long tot = group_sum<G>(local, gmask);
+        if (lane == 0 && tot) atomicAdd(p.sums, tot);
     }
 }
 
-// ---------------------------------------------------------------------------
-// block kinds: one item (row, mask chunk or column window, A-entry split) per CTA
-// ---------------------------------------------------------------------------
-template <int NT, int KIND, int CAP, int CHUNK, int SPLIT, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT) k_block(KArgs p) {
-    constexpr bool ACC = (EPI == EPI_WRITE);
-    constexpr int NW = NT / 32;
-    // MSA: CAP is log2 of the window width in columns
-    constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;
-    extern __shared__ int smem[];
-    __shared__ unsigned long long s_red[NW];
-    __shared__ int64_t s_item;
-    __shared__ int s_pos;
-    __shared__ int s_next;
-    const int lane = threadIdx.x & 31;
-    const int begin = p.voff[p.v], end = p.voff[p.v + 1];
-    if (begin == end) return;
-    const int64_t ibeg = p.item_ex[begin], iend = p.item_ex[end];
-    unsigned long long local = 0;
-
-    while (true) {
-        if (threadIdx.x == 0) {
-            const int64_t I = ibeg + static_cast<int64_t>(atomicAdd(p.fetch + p.v, 1u));
-            s_item = I;
-            if (I < iend) {  // last rowlist position whose prefix <= I
-                int lo = begin, hi = end;
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (p.item_ex[mid] <= I) lo = mid;
-                    else hi = mid;
-                }
-                s_pos = lo;
-            }
-        }
-        __syncthreads();
-        const int64_t I = s_item;
-        if (I >= iend) break;
-        const int pos = s_pos;
-        const int row = p.rowlist[pos];
-        const int64_t l = I - p.item_ex[pos];
-        const int64_t m0 = p.M.rp[row];
-        const int mlen = static_cast<int>(p.M.rp[row + 1] - m0);
-        const int64_t a0 = p.A.rp[row], alen = p.A.rp[row + 1] - a0;
-        const int64_t nsp = num_splits(p.work[row], alen, SPLIT);
-        const int64_t ch = l / nsp, sp = l % nsp;
-        const int64_t t0 = a0 + alen * sp / nsp, t1 = a0 + alen * (sp + 1) / nsp;
-        const int32_t *__restrict__ mc = p.M.col + m0;
-
-        // ---- build the mask structure of this item ----
-        int c0, c1;       // mask positions covered
-        int lo_col, hi_col;
-        int *keys = smem;
-        int *acc = smem + ((KIND == K_MSA_BLOCK) ? (ACC ? WIN / 32 : 0) : CAP);
-        unsigned *bits = reinterpret_cast<unsigned *>(smem);
-        bool cut;
-        if constexpr (KIND == K_MSA_BLOCK) {
-            const int64_t wbase = ((int64_t)(mc[0] >> CAP) + ch) << CAP;
-            lo_col = static_cast<int>(wbase);
-            { const int64_t hc = wbase + WIN - 1; hi_col = static_cast<int>(hc < 0x7FFFFFFF ? hc : 0x7FFFFFFF); }
-            // mask positions inside the window
-            int lo = 0, hi = mlen;
-            while (lo < hi) { const int md = (lo + hi) >> 1; if (mc[md] < lo_col) lo = md + 1; else hi = md; }
-            c0 = lo;
-            hi = mlen;
-            while (lo < hi) { const int md = (lo + hi) >> 1; if (mc[md] <= hi_col) lo = md + 1; else hi = md; }
-            c1 = lo;
-            for (int wd = threadIdx.x; wd < WIN / 32; wd += NT) bits[wd] = 0u;
-            __syncthreads();
-            for (int q = c0 + threadIdx.x; q < c1; q += NT) {
-                const int x = mc[q] - lo_col;
-                atomicOr(bits + (x >> 5), 1u << (x & 31));
-                if (ACC) acc[x] = 0;
-            }
-            cut = (mc[0] >> CAP) != (mc[mlen - 1] >> CAP);
-        } else {
-            const int CH = CHUNK;
-            c0 = static_cast<int>(ch) * CH;
-            c1 = min(mlen, c0 + CH);
-            if constexpr (KIND == K_MCA_BLOCK) {
-                for (int q = threadIdx.x; q < c1 - c0; q += NT) {
-                    keys[q] = mc[c0 + q];
-                    if (ACC) acc[q] = 0;
-                }
-            } else {
-                for (int s = threadIdx.x; s < CAP; s += NT) {
-                    keys[s] = EMPTY_KEY;
-                    if (ACC) acc[s] = 0;
-                }
-                __syncthreads();
-                for (int q = c0 + threadIdx.x; q < c1; q += NT) hash_insert<CAP>(keys, mc[q]);
-            }
-            lo_col = mc[c0];
-            hi_col = mc[c1 - 1];
-            cut = mlen > CH;
-        }
-        if (threadIdx.x == 0) s_next = static_cast<int>(0);
-        __syncthreads();
-
-        // ---- stream the B rows of A entries [t0, t1); warps fetch entries
-        //      dynamically, the next entry's bounds load during the current row ----
-        unsigned cnt = 0;
-        const int clen = c1 - c0;
-        if (c1 > c0) {
-            constexpr int PKV = (KIND == K_MSA_BLOCK) ? PK_MSA : ((KIND == K_MCA_BLOCK) ? PK_MCA : PK_HASH);
-            const int probe_arg = (KIND == K_MSA_BLOCK) ? lo_col : clen;
-            const int *pkeys = (KIND == K_MSA_BLOCK) ? reinterpret_cast<const int *>(bits) : keys;
-            auto fetch = [&]() -> int64_t {
-                int tt = 0;
-                if (lane == 0) tt = atomicAdd(&s_next, 1);
-                return t0 + __shfl_sync(0xFFFFFFFFu, tt, 0);
-            };
-            int64_t tc = fetch();
-            if (tc < t1) {
-                BRow nxt = brow_of<VAL>(p, __ldg(p.A.col + tc), tc);
-                int64_t tn = fetch();
-                int k2 = tn < t1 ? __ldg(p.A.col + tn) : 0;
-                while (tc < t1) {
-                    BRow cur = nxt;
-                    if (tn < t1) nxt = brow_of<VAL>(p, k2, tn);
-                    const int64_t tnn = (tn < t1) ? fetch() : t1;
-                    if (tnn < t1) k2 = __ldg(p.A.col + tnn);
-                    if (cur.b0 < cur.b1) {
-                        bool skip = false;
-                        if (cut) {
-                            skip = __ldg(p.B.col + cur.b1 - 1) < lo_col || __ldg(p.B.col + cur.b0) > hi_col;
-                            if (!skip) {
-                                const int64_t lo = group_lower_bound<32>(p.B.col, cur.b0, cur.b1, lo_col, lane,
-                                                                         0xFFFFFFFFu);
-                                cur.b1 = group_lower_bound<32>(p.B.col, lo, cur.b1, hi_col + 1, lane, 0xFFFFFFFFu);
-                                cur.b0 = lo;
-                            }
-                        }
-                        if (!skip)
-                            stream_row<32, CAP, PKV, ACC, VAL>(p, cur.b0, cur.b1, lane, cur.av, pkeys, acc, probe_arg,
-                                                               cnt);
-                    }
-                    tc = tn;
-                    tn = tnn;
-                }
-            }
-        }
-        __syncthreads();
-
-        // ---- epilogue ----
-        if (ACC) {
-            for (int q = c0 + threadIdx.x; q < c1; q += NT) {
-                int s;
-                if constexpr (KIND == K_MSA_BLOCK) s = mc[q] - lo_col;
-                else if constexpr (KIND == K_MCA_BLOCK) s = q - c0;
-                else s = hash_find<CAP>(keys, mc[q]);
-                const int val = acc[s];
-                if (nsp == 1) p.c_val[m0 + q] = val;
-                else if (val) atomicAdd(p.c_val + m0 + q, val);
-            }
-        } else if (EPI == EPI_KEYED) {
-            const unsigned long long tot = block_sum(static_cast<unsigned long long>(cnt), s_red);
-            if (threadIdx.x == 0 && tot) atomicAdd(p.sums + (p.row_key ? p.row_key[row] : row), tot);
-        } else {
-            local += cnt;
-        }
-        __syncthreads();
-    }
-    if (EPI == EPI_SUM) {
-        const unsigned long long tot = block_sum(local, s_red);
-        if (threadIdx.x == 0 && tot) atomicAdd(p.sums, tot);
-    }
-}
+#include "gk_kblock.cuh"
 
 // ---------------------------------------------------------------------------
 // host side: launching one variant
@@ -561,13 +501,15 @@ constexpr size_t smem_bytes(bool write) {
         const int nt = group_cta_threads(V);
         const int ng = nt / X.G;
         const int cap = (X.kind == K_MCA_GROUP) ? X.chunk : X.cap;
-        return size_t(ng) * cap * 4 * (write ? 2 : 1);
+        const size_t filter = (X.kind == K_HASH_GROUP && X.flog > 0) ? (size_t(1) << X.flog) / 8 : 0;
+        return size_t(ng) * (size_t(cap) * 4 * (write ? 2 : 1) + filter);
     } else if constexpr (X.kind == K_MSA_BLOCK) {
         if (write) return (size_t(1) << X.cap_write) / 8 + (size_t(1) << X.cap_write) * 4;
         return (size_t(1) << X.cap) / 8;
     } else {
         const int cap = write ? X.cap_write : X.cap;
-        return size_t(cap) * 4 * (write ? 2 : 1);
+        const size_t filter = (X.kind == K_HASH_BLOCK && X.flog > 0) ? (size_t(1) << X.flog) / 8 : 0;
+        return size_t(cap) * 4 * (write ? 2 : 1) + filter;
     }
 }
 
@@ -582,12 +524,13 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         constexpr int NTV = group_cta_threads(V);
         constexpr bool MCA = X.kind == K_MCA_GROUP;
         constexpr int CAPV = MCA ? X.chunk : X.cap;
-        fn = k_group<X.G, X.sub, NTV, CAPV, X.chunk, MCA, EPI, VAL>;
+        fn = k_group<X.G, X.sub, NTV, CAPV, X.chunk, MCA, (MCA ? 0 : X.flog), EPI, VAL>;
         nt = NTV;
     } else {
         constexpr int CAPV = W ? X.cap_write : X.cap;
         constexpr int CHV = W ? X.chunk_write : X.chunk;
-        fn = k_block<X.G, X.kind, CAPV, CHV, X.split_log2, EPI, VAL>;
+        constexpr int FLOGV = (X.kind == K_HASH_BLOCK) ? X.flog : 0;
+        fn = k_block<X.G, X.kind, X.sub, CAPV, CHV, X.split_log2, FLOGV, X.batch, EPI, VAL>;
         nt = X.G;
     }
     // resident CTAs per SM, computed once per kernel instance (and device)
@@ -662,12 +605,13 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     GK_CHECK(scr.alloc(&item_ex, m + 1));
     GK_CHECK(scr.alloc(&bins, NBINS));
     GK_CHECK(scr.alloc(&var_of_bin, NBINS));
-    GK_CHECK(scr.alloc(&vcount, 4 * NV + 4));
+    GK_CHECK(scr.alloc(&vcount, 6 * NV + 4));
     voff = vcount + NV;
-    vcursor = voff + NV + 1;
+    vcursor = voff + NV + 1;          // 2 * NV
+    int *vsimple = vcursor + 2 * NV;  // NV
     GK_CHECK(scr.alloc(&fetch, NV));
     GK_CUDA(cudaMemsetAsync(bins, 0, sizeof(BinStats) * NBINS, s));
-    GK_CUDA(cudaMemsetAsync(vcount, 0, sizeof(int) * (4 * NV + 4), s));
+    GK_CUDA(cudaMemsetAsync(vcount, 0, sizeof(int) * (6 * NV + 4), s));
     GK_CUDA(cudaMemsetAsync(item_n, 0, sizeof(int64_t) * (m + 1), s));
 
     const int sms = c.num_sms;
@@ -684,9 +628,9 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
         GK_CUDA(cudaMemcpyAsync(rq.bin_stats_out, bins, sizeof(BinStats) * NBINS, cudaMemcpyDeviceToDevice, s));
     if (rq.variant_of_bin_out && rq.force_variant < 0)
         GK_CUDA(cudaMemcpyAsync(rq.variant_of_bin_out, var_of_bin, sizeof(int) * NBINS, cudaMemcpyDeviceToDevice, s));
-    k_count_rows<<<sms * 2, 256, 0, s>>>(m, bin, var_of_bin, rq.force_variant, vcount);
+    k_count_rows<<<sms * 2, 256, 0, s>>>(A, M, work, bin, var_of_bin, rq.force_variant, write, vcount, vsimple);
     GK_CUDA(cudaGetLastError());
-    k_offsets<<<1, 32, 0, s>>>(vcount, voff, vcursor, fetch);
+    k_offsets<<<1, 32, 0, s>>>(vcount, vsimple, voff, vcursor, fetch);
     GK_CUDA(cudaGetLastError());
     k_scatter_rows<<<sms * 2, 256, 0, s>>>(A, M, work, bin, var_of_bin, rq.force_variant, write, vcursor,
                                            rowlist, item_n);
@@ -705,6 +649,7 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     args.M = M;
     args.rowlist = rowlist;
     args.voff = voff;
+    args.vsimple = vsimple;
     args.item_ex = item_ex;
     args.work = work;
     args.fetch = fetch;
@@ -713,10 +658,15 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     args.row_key = rq.row_key;
     args.vec = (reinterpret_cast<uintptr_t>(B.col) % 16) == 0;
     const bool val = rq.use_values && (A.val || B.val);
-    // the variant kernels are independent: fork them onto side streams so
-    // that one variant's tail overlaps the others, then join (capturable)
+    // the variant kernels are independent: with GK_CONCURRENT_VARIANTS=1 they
+    // are forked onto side streams and joined (capturable).  Off by default:
+    // each variant is a persistent grid that fills the GPU by itself.
+    static const bool concurrent = [] {
+        const char *e = getenv("GK_CONCURRENT_VARIANTS");
+        return e && e[0] == '1';
+    }();
     SideStreams &side = side_streams();
-    const bool fork = rq.force_variant < 0;
+    const bool fork = concurrent && rq.force_variant < 0;
     if (fork) GK_CUDA(cudaEventRecord(side.fork, s));
     ProfWindow prof(s, NV);
     for (int v = 0; v < NV; ++v) {
