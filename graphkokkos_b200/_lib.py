@@ -101,6 +101,13 @@ SIGNATURES = {
     "gk_sched_model_size": (ctypes.c_size_t, []),
     "gk_sched_set_model": (ctypes.c_int, [VP, ctypes.c_size_t]),
     "gk_sched_has_model": (ctypes.c_int, []),
+    "gk_sched_num_bins": (ctypes.c_int, []),
+    "gk_sched_variant_allowed": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "gk_sched_bins": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, VP, VP, VP, VP]),
+    "gk_tune_run": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, VP, VP, VP]),
+    "gk_mlp_loss_grad": (ctypes.c_int, [VP, VP, VP, VP, ctypes.c_int, VP, VP, VP]),
+    "gk_mlp_train": (ctypes.c_int, [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_float, VP, VP]),
+    "gk_mlp_forward": (ctypes.c_int, [VP, VP, ctypes.c_int, VP, VP]),
     "gk_prof_enable": (ctypes.c_int, [ctypes.c_int]),
     "gk_prof_count": (ctypes.c_int, []),
     "gk_prof_flush": (ctypes.c_int, []),

@@ -74,6 +74,30 @@ __host__ __device__ constexpr int group_cta_threads(int) { return NT_GROUP; }
 // variant ids the heuristics name
 constexpr int V_MCA_GROUP = 9, V_MCA_BLOCK = 10, V_MSA_BLOCK = 11;
 
+// Variants the learned scheduler (and the autotuner) may pick for a bin: a
+// variant is excluded where it would split every mask row into many chunks
+// (small structures on long mask rows) or rebuild a large structure for every
+// short row (large structures on short mask rows).
+__host__ __device__ constexpr bool variant_allowed(int v, int bin) {
+    const int qm = bin / NB_B;  // floor(log2(nnz(M_i)))
+    switch (v) {
+        case 0: return qm <= 5;
+        case 1: return qm <= 6;
+        case 2: return qm <= 8;
+        case 3: return qm <= 10;
+        case 4:
+        case 5: return qm <= 11;
+        case 6: return true;
+        case 7: return qm >= 5;
+        case 8: return qm >= 8;
+        case 9: return qm <= 9;
+        case 10: return qm >= 7;
+        case 11: return qm >= 9;
+        case 12: return qm >= 5;
+        default: return false;
+    }
+}
+
 // ---- features of a bin (inputs of the learned scheduler) ---------------------
 constexpr int NFEAT = 8;
 // f0 log2(1+mean nnz(M_i))   f1 log2(1+mean nnz(B_k))   f2 log2(1+mean nnz(A_i))

@@ -31,6 +31,8 @@ struct SpgemmRequest {
     // optional outputs for the scheduler and the autotuner
     BinStats *bin_stats_out = nullptr;  // device [NBINS]
     int *variant_of_bin_out = nullptr;  // device [NBINS]
+    float *variant_ms_out = nullptr;    // host [NV]: CUDA-event time of each variant launch (synchronises)
+    bool stats_only = false;            // stop after the bin statistics
 };
 
 int run_spgemm(const SpgemmRequest &req, Scratch &scr);

@@ -67,7 +67,7 @@ __host__ __device__ inline int forced_variant(int bin, const BinStats &b, int ac
     }
 }
 
-__device__ inline int mlp_variant(const float *w, const float *f_raw) {
+__device__ inline int mlp_variant(const float *w, const float *f_raw, int bin) {
     const float *W1 = w;
     const float *b1 = W1 + MLP_H * NFEAT;
     const float *W2 = b1 + MLP_H;
@@ -88,9 +88,10 @@ __device__ inline int mlp_variant(const float *w, const float *f_raw) {
         for (int i = 0; i < MLP_H; ++i) a += W2[j * MLP_H + i] * h1[i];
         h2[j] = a > 0.f ? a : 0.f;
     }
-    int best = 0;
+    int best = 6;  // allowed for every bin
     float best_s = 3.0e38f;
     for (int v = 0; v < NV; ++v) {
+        if (!variant_allowed(v, bin)) continue;
         float a = b3[v];
         for (int i = 0; i < MLP_H; ++i) a += W3[v * MLP_H + i] * h2[i];
         if (a < best_s) {
@@ -114,10 +115,13 @@ __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int ac
     else if (mode == GK_SCHED_LEARNED) {
         float f[NFEAT];
         bin_features(st, epi, values, f);
-        v = mlp_variant(d_mlp, f);
+        v = mlp_variant(d_mlp, f, b);
     } else v = plain_variant(b, st);
     var_of_bin[b] = v;
 }
+
+void bin_features_host(const BinStats &b, int epi, bool values, float *f) { bin_features(b, epi, values, f); }
+int plain_variant_host(int bin, const BinStats &b) { return plain_variant(bin, b); }
 
 static int ensure_model_on_device() {
     int dev = 0;
@@ -146,6 +150,9 @@ int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_acc
 extern "C" {
 
 int gk_sched_num_variants(void) { return gk::NV; }
+int gk_sched_variant_allowed(int bin, int variant) {
+    return (bin >= 0 && bin < gk::NBINS && gk::variant_allowed(variant, bin)) ? 1 : 0;
+}
 int gk_sched_num_features(void) { return gk::NFEAT; }
 size_t gk_sched_model_size(void) { return static_cast<size_t>(gk::MLP_SIZE); }
 

@@ -628,6 +628,10 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
         GK_CUDA(cudaMemcpyAsync(rq.bin_stats_out, bins, sizeof(BinStats) * NBINS, cudaMemcpyDeviceToDevice, s));
     if (rq.variant_of_bin_out && rq.force_variant < 0)
         GK_CUDA(cudaMemcpyAsync(rq.variant_of_bin_out, var_of_bin, sizeof(int) * NBINS, cudaMemcpyDeviceToDevice, s));
+    if (rq.stats_only) {
+        note_launches(2);
+        return GK_OK;
+    }
     k_count_rows<<<sms * 2, 256, 0, s>>>(A, M, work, bin, var_of_bin, rq.force_variant, write, vcount, vsimple);
     GK_CUDA(cudaGetLastError());
     k_offsets<<<1, 32, 0, s>>>(vcount, vsimple, voff, vcursor, fetch);
@@ -669,8 +673,17 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     const bool fork = concurrent && rq.force_variant < 0;
     if (fork) GK_CUDA(cudaEventRecord(side.fork, s));
     ProfWindow prof(s, NV);
+    cudaEvent_t tev[NV + 1];
+    const bool timed = rq.variant_ms_out != nullptr;
+    if (timed) {
+        for (int v = 0; v <= NV; ++v) GK_CUDA(cudaEventCreate(&tev[v]));
+        GK_CUDA(cudaEventRecord(tev[0], s));
+    }
     for (int v = 0; v < NV; ++v) {
-        if (rq.force_variant >= 0 && v != rq.force_variant) continue;
+        if (rq.force_variant >= 0 && v != rq.force_variant) {
+            if (timed) GK_CUDA(cudaEventRecord(tev[v + 1], s));
+            continue;
+        }
         args.v = v;
         cudaStream_t vs = s;
         if (fork) {
@@ -686,6 +699,16 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
             GK_CUDA(cudaEventRecord(side.join[v], vs));
             GK_CUDA(cudaStreamWaitEvent(s, side.join[v], 0));
         }
+        if (timed) GK_CUDA(cudaEventRecord(tev[v + 1], s));
+    }
+    if (timed) {
+        GK_CUDA(cudaEventSynchronize(tev[NV]));
+        for (int v = 0; v < NV; ++v) {
+            float ms = 0.f;
+            GK_CUDA(cudaEventElapsedTime(&ms, tev[v], tev[v + 1]));
+            rq.variant_ms_out[v] = ms;
+        }
+        for (int v = 0; v <= NV; ++v) cudaEventDestroy(tev[v]);
     }
     if (prof.active()) {
         // attribute the bins' work to the variants that ran them

@@ -1,0 +1,323 @@
+"""Learned row-bin scheduler: autotuner sweep, MLP training on the GPU, model I/O.
+
+The masked SpGEMM engine bins the rows of C<M> = A·B by (log2 nnz(M_i),
+log2 mean nnz(B_k)) and runs every bin on one kernel variant (include/gk_b200.h,
+graphkokkos_b200/csrc/gk_sched.cuh).  This module
+
+  * sweeps: for every bin of a graph with enough work and every variant the
+    bin admits, times that bin alone on that variant (gk_tune_run; CUDA events
+    around the variant kernel);
+  * builds the training set: per bin the 8 features the model reads
+    (gk_sched_bins) and, per variant, log2 of nanoseconds per streamed B entry;
+  * trains the MLP with the library's CUDA training kernel (gk_mlp_train);
+  * saves / loads the model (graphkokkos_b200/sched/model.npz) and hands it to
+    the library (gk_sched_set_model).
+
+The model changes only which variant runs a bin; every variant computes the
+same integer terms, so results stay bit-exact.
+
+  python -m graphkokkos_b200.sched --train          # sweep the training graphs, train, save
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MODEL_DIR = os.path.join(HERE, "sched")
+MODEL_PATH = os.path.join(MODEL_DIR, "model.npz")
+DATA_PATH = os.path.join(MODEL_DIR, "sweep.npz")
+
+MLP_H = 32
+
+
+def dims():
+    lib = _lib.load()
+    return int(lib.gk_sched_num_variants()), int(lib.gk_sched_num_features()), int(lib.gk_sched_num_bins())
+
+
+def model_size():
+    return int(_lib.load().gk_sched_model_size())
+
+
+# ---------------------------------------------------------------------------
+# model I/O
+# ---------------------------------------------------------------------------
+def load_model(path=MODEL_PATH):
+    w = np.ascontiguousarray(np.load(path)["w"], dtype=np.float32)
+    check(_lib.load().gk_sched_set_model(w.ctypes.data, w.shape[0]))
+    return w
+
+
+def save_model(w, path=MODEL_PATH, **meta):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, w=np.asarray(w, dtype=np.float32), meta=json.dumps(meta))
+
+
+# ---------------------------------------------------------------------------
+# bins and the sweep
+# ---------------------------------------------------------------------------
+def bins(G, mode):
+    """Per-bin statistics (rows, sum_m, sum_a, sum_work, max_b), plain choice and
+    features of C<G> = G·G (mode 0: triangle counting on L; mode 1: k-truss support)."""
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    stats = np.zeros((nb, 5), dtype=np.int64)
+    plain = np.zeros(nb, dtype=np.int32)
+    feats = np.zeros((nb, nf), dtype=np.float32)
+    g = G.as_gk()
+    check(lib.gk_sched_bins(ctypes.byref(g), mode, stats.ctypes.data, plain.ctypes.data, None, feats.ctypes.data,
+                            _stream(G)))
+    return stats, plain, feats
+
+
+def learned_choice(G, mode):
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    stats = np.zeros((nb, 5), dtype=np.int64)
+    learned = np.zeros(nb, dtype=np.int32)
+    g = G.as_gk()
+    check(lib.gk_sched_bins(ctypes.byref(g), mode, stats.ctypes.data, None, learned.ctypes.data, None, _stream(G)))
+    return learned
+
+
+def allowed(b, v):
+    return bool(_lib.load().gk_sched_variant_allowed(int(b), int(v)))
+
+
+def _stream(G):
+    try:
+        import torch
+        if G.is_cuda:
+            return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    except Exception:
+        pass
+    return ctypes.c_void_p(0)
+
+
+def time_bin(G, mode, b, v, reps=2):
+    """Best-of-reps CUDA-event time (ms) of bin b's rows on variant v."""
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    table = np.full(nb, -1, dtype=np.int32)
+    table[b] = v
+    ms = np.zeros(nv, dtype=np.float32)
+    g = G.as_gk()
+    best = float("inf")
+    for _ in range(reps):
+        check(lib.gk_tune_run(ctypes.byref(g), mode, table.ctypes.data, ms.ctypes.data, None, _stream(G)))
+        best = min(best, float(ms[v]))
+    return best
+
+
+def sweep(G, mode, name, min_work=1 << 20, reps=2, log=print):
+    """Times every admissible (bin, variant) pair of a graph; returns a list of
+    records {graph, mode, bin, features, rows, work, plain, ms: {variant: ms}}."""
+    nv, nf, nb = dims()
+    stats, plain, feats = bins(G, mode)
+    recs = []
+    t0 = time.time()
+    for b in range(nb):
+        rows, _, _, work, _ = stats[b]
+        if rows == 0 or work < min_work:
+            continue
+        ms = {}
+        for v in range(nv):
+            if allowed(b, v):
+                ms[v] = time_bin(G, mode, b, v, reps)
+        recs.append(dict(graph=name, mode=mode, bin=b, features=feats[b].tolist(), rows=int(rows), work=int(work),
+                         plain=int(plain[b]), ms={int(k): float(x) for k, x in ms.items()}))
+        best = min(ms, key=ms.get)
+        log(f"  {name} bin {b:3d} (qm {b // 16:2d} qb {b % 16:2d}) rows {rows:9d} work {work:.3e}  plain v{plain[b]} "
+            f"{ms.get(int(plain[b]), float('nan')):8.3f} ms  best v{best} {ms[best]:8.3f} ms")
+    log(f"  {name}: {len(recs)} bins in {time.time() - t0:.1f} s")
+    return recs
+
+
+def to_dataset(recs):
+    nv, nf, nb = dims()
+    X = np.zeros((len(recs), nf), dtype=np.float32)
+    Y = np.zeros((len(recs), nv), dtype=np.float32)
+    M = np.zeros((len(recs), nv), dtype=np.float32)
+    for i, r in enumerate(recs):
+        X[i] = r["features"]
+        for v, ms in r["ms"].items():
+            Y[i, v] = np.log2(max(ms, 1e-4) * 1e6 / r["work"])  # log2 ns per streamed B entry
+            M[i, v] = 1.0
+    return X, Y, M
+
+
+# ---------------------------------------------------------------------------
+# model
+# ---------------------------------------------------------------------------
+def init_weights(X, seed=0):
+    nv, nf, nb = dims()
+    rng = np.random.default_rng(seed)
+    parts = [
+        rng.normal(0, np.sqrt(2.0 / nf), (MLP_H, nf)), np.zeros(MLP_H),
+        rng.normal(0, np.sqrt(2.0 / MLP_H), (MLP_H, MLP_H)), np.zeros(MLP_H),
+        rng.normal(0, np.sqrt(1.0 / MLP_H), (nv, MLP_H)), np.zeros(nv),
+        X.mean(axis=0), np.maximum(X.std(axis=0), 1e-3),
+    ]
+    w = np.concatenate([np.ravel(p) for p in parts]).astype(np.float32)
+    assert w.shape[0] == model_size()
+    return w
+
+
+def mean_target(Y, M):
+    """Output bias initialised to the mean measured cost of each variant."""
+    s = (Y * M).sum(axis=0)
+    c = M.sum(axis=0)
+    return np.where(c > 0, s / np.maximum(c, 1), 0.0)
+
+
+def train(X, Y, M, epochs=4000, lr=3e-3, seed=0):
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    w = init_weights(X, seed)
+    w[-(2 * nf + nv):-2 * nf] = mean_target(Y, M)
+    trace = np.zeros(epochs, dtype=np.float32)
+    X, Y, M = (np.ascontiguousarray(a, dtype=np.float32) for a in (X, Y, M))
+    check(lib.gk_mlp_train(w.ctypes.data, X.ctypes.data, Y.ctypes.data, M.ctypes.data, X.shape[0], epochs,
+                           ctypes.c_float(lr), trace.ctypes.data, None))
+    return w, trace
+
+
+def forward_gpu(w, X):
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.zeros((X.shape[0], nv), dtype=np.float32)
+    check(lib.gk_mlp_forward(np.ascontiguousarray(w, dtype=np.float32).ctypes.data, X.ctypes.data, X.shape[0],
+                             out.ctypes.data, None))
+    return out
+
+
+def forward_numpy(w, X, nf, nv):
+    """The network in numpy (same layout as the CUDA kernels)."""
+    h = MLP_H
+    o = 0
+    W1 = w[o:o + h * nf].reshape(h, nf); o += h * nf
+    b1 = w[o:o + h]; o += h
+    W2 = w[o:o + h * h].reshape(h, h); o += h * h
+    b2 = w[o:o + h]; o += h
+    W3 = w[o:o + nv * h].reshape(nv, h); o += nv * h
+    b3 = w[o:o + nv]; o += nv
+    mu = w[o:o + nf]; o += nf
+    sg = w[o:o + nf]
+    x = (X - mu) / sg
+    h1 = np.maximum(x @ W1.T + b1, 0)
+    h2 = np.maximum(h1 @ W2.T + b2, 0)
+    return h2 @ W3.T + b3
+
+
+def choose(out, recs):
+    """argmin over each bin's admissible variants (as the device inference does)."""
+    picks = []
+    for i, r in enumerate(recs):
+        cand = [v for v in range(out.shape[1]) if allowed(r["bin"], v)]
+        picks.append(min(cand, key=lambda v: out[i, v]))
+    return picks
+
+
+def evaluate(recs, picks):
+    """Measured time of the plain heuristic's, the model's and the best choices,
+    summed over the bins (a pick without a measurement counts as the bin's
+    slowest measured time)."""
+    plain = learned = best = 0.0
+    for r, p in zip(recs, picks):
+        ms = r["ms"]
+        worst = max(ms.values())
+        plain += ms.get(r["plain"], worst)
+        learned += ms.get(p, worst)
+        best += min(ms.values())
+    return dict(plain_ms=plain, learned_ms=learned, best_ms=best)
+
+
+def save_dataset(recs, path=DATA_PATH):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez_compressed(path, records=json.dumps(recs))
+
+
+def load_dataset(path=DATA_PATH):
+    recs = json.loads(str(np.load(path)["records"]))
+    for r in recs:  # JSON object keys are strings
+        r["ms"] = {int(k): float(v) for k, v in r["ms"].items()}
+    return recs
+
+
+# ---------------------------------------------------------------------------
+# training graphs (seeds differ from the benchmark graphs')
+# ---------------------------------------------------------------------------
+TRAIN_GRAPHS = [
+    ("rmat16-s11", dict(kind="rmat", scale=16, seed=11)),
+    ("rmat18-s12", dict(kind="rmat", scale=18, seed=12)),
+    ("rmat20-s13", dict(kind="rmat", scale=20, seed=13)),
+    ("rmat22-s14", dict(kind="rmat", scale=22, seed=14)),
+    ("rmat24-s15", dict(kind="rmat", scale=24, seed=15)),
+    ("er1m-d16-s16", dict(kind="er", n=1 << 20, nedges=8 << 20, seed=16)),
+    ("er4m-d32-s17", dict(kind="er", n=1 << 22, nedges=64 << 20, seed=17)),
+]
+KTRUSS_GRAPHS = [
+    ("rmat18-s18", dict(kind="rmat", scale=18, seed=18)),
+    ("rmat20-s19", dict(kind="rmat", scale=20, seed=19)),
+]
+
+
+def build_graph(spec):
+    from . import api
+    if spec["kind"] == "rmat":
+        return api.gen_rmat(spec["scale"], 16, seed=spec["seed"], device="cuda")
+    return api.gen_er(spec["n"], spec["nedges"], seed=spec["seed"], device="cuda")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", action="store_true", help="sweep the training graphs, train and save the model")
+    ap.add_argument("--retrain", action="store_true", help="train from the saved sweep without re-measuring")
+    ap.add_argument("--epochs", type=int, default=4000)
+    ap.add_argument("--max-scale", type=int, default=24)
+    ap.add_argument("--out", default=MODEL_DIR, help="directory for model.npz (and sweep.npz with --train)")
+    ap.add_argument("--data", default=DATA_PATH, help="sweep to train from with --retrain")
+    args = ap.parse_args()
+    model_path = os.path.join(args.out, "model.npz")
+    data_path = os.path.join(args.out, "sweep.npz") if args.train else args.data
+    import torch
+    from . import api
+    torch.cuda.set_device(0)
+    if args.train:
+        recs = []
+        for name, spec in TRAIN_GRAPHS:
+            if spec.get("scale", 0) > args.max_scale:
+                continue
+            A = build_graph(spec)
+            L = api.extract_lower(A)
+            del A
+            recs += sweep(L, 0, name)
+            del L
+            torch.cuda.empty_cache()
+        for name, spec in KTRUSS_GRAPHS:
+            A = build_graph(spec)
+            recs += sweep(A, 1, name + "-ktruss")
+            del A
+            torch.cuda.empty_cache()
+        save_dataset(recs, data_path)
+    recs = load_dataset(data_path)
+    X, Y, M = to_dataset(recs)
+    w, trace = train(X, Y, M, epochs=args.epochs)
+    picks = choose(forward_gpu(w, X), recs)
+    ev = evaluate(recs, picks)
+    print(json.dumps({"samples": len(recs), "loss_first": float(trace[0]), "loss_last": float(trace[-1]), **ev}))
+    save_model(w, model_path, samples=len(recs), epochs=args.epochs, final_loss=float(trace[-1]), **ev)
+
+
+if __name__ == "__main__":
+    main()

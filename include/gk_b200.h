@@ -179,6 +179,44 @@ size_t gk_sched_model_size(void);
 int gk_sched_set_model(const float *weights, size_t n_floats);
 int gk_sched_has_model(void);
 
+/* ----- autotuning and training of the learned scheduler (no reference
+ * counterpart: the reference's only scheduling is the CLI's per-call accumulator
+ * choice, src/main.cpp:194-212) ------------------------------------------------ */
+
+/* Per-bin statistics of the rows of a product: the rows' count, summed mask /
+ * A entries, summed streamed B entries (work) and the longest B row seen. */
+typedef struct gk_bin_stat {
+    int64_t rows, sum_m, sum_a, sum_work, max_b;
+} gk_bin_stat;
+int gk_sched_num_bins(void);
+/* 1 if the learned scheduler may place `bin` on `variant` (0 otherwise). */
+int gk_sched_variant_allowed(int bin, int variant);
+
+/* mode 0: triangle counting on L (A = B = M = L, sum of C); mode 1: k-truss
+ * support on a symmetric A (A = B = M = A, values written).  Fills, per bin,
+ * the statistics, the plain heuristic's variant (or -1 for an empty bin), the
+ * learned model's variant (NULL to skip; needs a loaded model) and the
+ * gk_sched_num_features() features the model reads (NULL to skip). */
+int gk_sched_bins(const gk_csr *G, int mode, gk_bin_stat *stats, int32_t *plain_variant, int32_t *learned_variant,
+                  float *features, void *stream);
+
+/* Runs the product of `mode` with bin b's rows on variant bin_variant[b]
+ * (-1: rows skipped) and returns each variant kernel's CUDA-event time in
+ * variant_ms[gk_sched_num_variants()] (synchronises); *sum (mode 0) receives
+ * the partial sum of C over the rows that ran. */
+int gk_tune_run(const gk_csr *G, int mode, const int32_t *bin_variant, float *variant_ms, uint64_t *sum,
+                void *stream);
+
+/* MLP of the learned scheduler, trained on the GPU by hand-written kernels.
+ * w: gk_sched_model_size() floats (layout in graphkokkos_b200/csrc/gk_sched.cuh);
+ * X: n x gk_sched_num_features(); Y, mask: n x gk_sched_num_variants() targets
+ * (log2 ns per streamed B entry) and 0/1 weights.  All arrays are host memory. */
+int gk_mlp_loss_grad(const float *w, const float *X, const float *Y, const float *mask, int n, float *loss,
+                     float *grad, void *stream);
+int gk_mlp_train(float *w, const float *X, const float *Y, const float *mask, int n, int epochs, float lr,
+                 float *loss_trace, void *stream);
+int gk_mlp_forward(const float *w, const float *X, int n, float *out, void *stream);
+
 /* ----- profiling (no reference counterpart; the reference prints chrono
  * brackets, src/main.cpp:74-86) -------------------------------------------------- */
 

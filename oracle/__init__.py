@@ -151,6 +151,19 @@ def bc_f64(A, sources):
     return out
 
 
+def mlp_loss_grad(w, X, Y, M, F, H, V):
+    """FP64 loss and gradient of the scheduler MLP (checker of gk_mlp_loss_grad)."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.ascontiguousarray(Y, dtype=np.float32)
+    M = np.ascontiguousarray(M, dtype=np.float32)
+    grad = np.zeros(w.shape[0], dtype=np.float64)
+    loss = ctypes.c_double(0.0)
+    port().orc_mlp_loss_grad(ctypes.c_int(F), ctypes.c_int(H), ctypes.c_int(V), _p(w), _p(X), _p(Y), _p(M),
+                             ctypes.c_int(X.shape[0]), ctypes.byref(loss), _p(grad))
+    return float(loss.value), grad
+
+
 def transpose(A):
     m, n, rp, col, val = _host(A)
     orp = np.zeros(n + 1, dtype=np.int64)

@@ -263,6 +263,72 @@ int orc_ktruss(int64_t m, const int64_t *rp, const int32_t *col, int k,
 }
 
 // ---------------------------------------------------------------------------
+// MLP of the learned scheduler, FP64 (checker of the CUDA training kernels;
+// the network has no reference counterpart).  Layout: W1[H][F], b1[H],
+// W2[H][H], b2[H], W3[V][H], b3[V], mu[F], sigma[F]; x = (f-mu)/sigma,
+// two ReLU layers, linear output; loss = sum over measured (sample, output)
+// pairs of squared error / their count.  grad has the layout of w (zeros for
+// mu and sigma).
+// ---------------------------------------------------------------------------
+int orc_mlp_loss_grad(int F, int H, int V, const float *w, const float *X, const float *Y, const float *M, int n,
+                      double *loss, double *grad) {
+    const int pW1 = 0, pB1 = pW1 + H * F, pW2 = pB1 + H, pB2 = pW2 + H * H, pW3 = pB2 + H, pB3 = pW3 + V * H,
+              pMU = pB3 + V, pSG = pMU + F, total = pSG + F;
+    std::fill(grad, grad + total, 0.0);
+    double count = 0;
+    for (int i = 0; i < n * V; ++i) count += M[i] > 0.f ? 1.0 : 0.0;
+    const double scale = count > 0 ? 1.0 / count : 0.0;
+    double se = 0;
+    std::vector<double> x(F), h1(H), h2(H), out(V), dout(V), dh2(H), dh1(H);
+    for (int s = 0; s < n; ++s) {
+        const float *f = X + static_cast<size_t>(s) * F;
+        for (int i = 0; i < F; ++i) x[i] = (static_cast<double>(f[i]) - w[pMU + i]) / w[pSG + i];
+        for (int j = 0; j < H; ++j) {
+            double a = w[pB1 + j];
+            for (int i = 0; i < F; ++i) a += static_cast<double>(w[pW1 + j * F + i]) * x[i];
+            h1[j] = a > 0 ? a : 0;
+        }
+        for (int j = 0; j < H; ++j) {
+            double a = w[pB2 + j];
+            for (int i = 0; i < H; ++i) a += static_cast<double>(w[pW2 + j * H + i]) * h1[i];
+            h2[j] = a > 0 ? a : 0;
+        }
+        for (int v = 0; v < V; ++v) {
+            double a = w[pB3 + v];
+            for (int i = 0; i < H; ++i) a += static_cast<double>(w[pW3 + v * H + i]) * h2[i];
+            out[v] = a;
+            const double e = M[static_cast<size_t>(s) * V + v] > 0.f ? a - Y[static_cast<size_t>(s) * V + v] : 0.0;
+            se += e * e;
+            dout[v] = 2 * e * scale;
+        }
+        for (int v = 0; v < V; ++v) {
+            grad[pB3 + v] += dout[v];
+            for (int i = 0; i < H; ++i) grad[pW3 + v * H + i] += dout[v] * h2[i];
+        }
+        for (int i = 0; i < H; ++i) {
+            double a = 0;
+            for (int v = 0; v < V; ++v) a += static_cast<double>(w[pW3 + v * H + i]) * dout[v];
+            dh2[i] = h2[i] > 0 ? a : 0;
+        }
+        for (int j = 0; j < H; ++j) {
+            grad[pB2 + j] += dh2[j];
+            for (int i = 0; i < H; ++i) grad[pW2 + j * H + i] += dh2[j] * h1[i];
+        }
+        for (int i = 0; i < H; ++i) {
+            double a = 0;
+            for (int j = 0; j < H; ++j) a += static_cast<double>(w[pW2 + j * H + i]) * dh2[j];
+            dh1[i] = h1[i] > 0 ? a : 0;
+        }
+        for (int j = 0; j < H; ++j) {
+            grad[pB1 + j] += dh1[j];
+            for (int i = 0; i < F; ++i) grad[pW1 + j * F + i] += dh1[j] * x[i];
+        }
+    }
+    *loss = se * scale;
+    return total;
+}
+
+// ---------------------------------------------------------------------------
 // Batched betweenness centrality in FP64: the algebra of
 // betweenness_centrality_batch (betweenness_centrality.h:406-506) with path
 // counts and dependencies in double and an explicit source list (the

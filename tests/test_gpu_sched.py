@@ -1,0 +1,124 @@
+"""The learned scheduler on the GPU: the hand-written CUDA MLP kernels against
+the FP64 CPU oracle (gradient check), training convergence, inference parity,
+and bit-exact results under the learned schedule."""
+import numpy as np
+import pytest
+
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+def random_problem(n, seed):
+    from graphkokkos_b200 import sched
+    nv, nf, nb = sched.dims()
+    rng = np.random.default_rng(seed)
+    X = rng.normal(0, 2, (n, nf)).astype(np.float32)
+    Y = rng.normal(0, 1, (n, nv)).astype(np.float32)
+    M = (rng.random((n, nv)) < 0.7).astype(np.float32)
+    w = sched.init_weights(X, seed)
+    w += rng.normal(0, 0.05, w.shape).astype(np.float32)
+    w[-2 * nf:] = np.concatenate([X.mean(0), X.std(0)])  # keep sigma positive
+    return w, X, Y, M
+
+
+def test_mlp_gradient_matches_fp64_oracle(gk, orc, cuda):
+    import ctypes
+    from graphkokkos_b200 import sched
+    nv, nf, nb = sched.dims()
+    lib = gk.load()
+    for seed, n in [(1, 7), (2, 300), (3, 1000)]:
+        w, X, Y, M = random_problem(n, seed)
+        loss = ctypes.c_float(0)
+        grad = np.zeros_like(w)
+        assert lib.gk_mlp_loss_grad(w.ctypes.data, X.ctypes.data, Y.ctypes.data, M.ctypes.data, n,
+                                    ctypes.addressof(loss), grad.ctypes.data, None) == 0
+        ref_loss, ref_grad = orc.mlp_loss_grad(w, X, Y, M, nf, sched.MLP_H, nv)
+        assert loss.value == pytest.approx(ref_loss, rel=1e-4)
+        scale = np.abs(ref_grad).max()
+        np.testing.assert_allclose(grad, ref_grad, rtol=2e-3, atol=2e-4 * scale)
+
+
+def test_mlp_gradient_finite_difference(orc):
+    """The FP64 oracle itself against central differences."""
+    from graphkokkos_b200 import sched
+    nv, nf, nb = sched.dims()
+    w, X, Y, M = random_problem(40, 9)
+    _, g = orc.mlp_loss_grad(w, X, Y, M, nf, sched.MLP_H, nv)
+    rng = np.random.default_rng(0)
+    ok = 0
+    idx = rng.choice(w.shape[0] - 2 * nf, 40, replace=False)
+    for i in idx:
+        h = 1e-3
+        wp, wm = w.copy(), w.copy()
+        wp[i] += h
+        wm[i] -= h
+        lp, _ = orc.mlp_loss_grad(wp, X, Y, M, nf, sched.MLP_H, nv)
+        lm, _ = orc.mlp_loss_grad(wm, X, Y, M, nf, sched.MLP_H, nv)
+        fd = (lp - lm) / float(wp[i] - wm[i])  # the float32 step actually taken
+        ok += fd == pytest.approx(g[i], rel=2e-2, abs=1e-4)
+    # a perturbation that crosses a ReLU kink makes the difference quotient
+    # disagree with the derivative; all but a few samples must agree
+    assert ok >= len(idx) - 2
+
+
+def test_mlp_forward_and_training(gk, cuda):
+    from graphkokkos_b200 import sched
+    nv, nf, nb = sched.dims()
+    rng = np.random.default_rng(5)
+    X = rng.normal(0, 1, (400, nf)).astype(np.float32)
+    # a learnable target: each variant's cost is a different function of the features
+    Y = np.stack([np.sin(X[:, v % nf]) + 0.3 * X[:, (v + 1) % nf] for v in range(nv)], 1).astype(np.float32)
+    M = np.ones_like(Y)
+    w, trace = sched.train(X, Y, M, epochs=1500, lr=3e-3)
+    assert trace[-1] < 0.25 * trace[0]
+    out_gpu = sched.forward_gpu(w, X)
+    out_np = sched.forward_numpy(w.astype(np.float64), X.astype(np.float64), nf, nv)
+    np.testing.assert_allclose(out_gpu, out_np, rtol=1e-4, atol=1e-4)
+
+
+def test_learned_schedule_is_bit_exact(gk, orc, cuda):
+    import os
+    from graphkokkos_b200 import sched
+    if not os.path.exists(sched.MODEL_PATH):
+        pytest.skip("no trained model committed")
+    sched.load_model()
+    for scale, seed in [(10, 1), (14, 1), (16, 3)]:
+        A = gk.gen_rmat(scale, 16, seed=seed, device="cuda")
+        L = gk.extract_lower(A)
+        want = orc.tc_lower(L.numpy())
+        assert gk.tc_count(L, sched="learned") == want
+        assert gk.tc_count(L, sched="plain") == want
+    A = gk.gen_rmat(11, 16, seed=7)
+    rp, col, iters, _ = orc.ktruss(A, 5)
+    T, it = gk.ktruss(A.to("cuda"), 5, sched="learned")
+    assert it == iters and np.array_equal(T.col.cpu().numpy(), col)
+    M = G.random_csr(300, 250, 0.05, 1, values=True)
+    B = G.random_csr(250, 280, 0.05, 2, values=True)
+    Mk = G.random_csr(300, 280, 0.1, 3)
+    np.testing.assert_array_equal(
+        gk.mxmm_masked(M.to("cuda"), B.to("cuda"), Mk.to("cuda"), sched="learned").cpu().numpy(),
+        orc.mxmm(M, B, Mk))
+
+
+def test_learned_choices_match_numpy_inference(gk, cuda):
+    import os
+    from graphkokkos_b200 import sched
+    if not os.path.exists(sched.MODEL_PATH):
+        pytest.skip("no trained model committed")
+    w = sched.load_model()
+    nv, nf, nb = sched.dims()
+    A = gk.gen_rmat(18, 16, seed=2, device="cuda")
+    L = gk.extract_lower(A)
+    stats, plain, feats = sched.bins(L, 0)
+    learned = sched.learned_choice(L, 0)
+    out = sched.forward_numpy(w.astype(np.float64), feats.astype(np.float64), nf, nv)
+    for b in range(nb):
+        if stats[b, 0] == 0:
+            continue
+        cand = [v for v in range(nv) if sched.allowed(b, v)]
+        scores = out[b, cand]
+        best = cand[int(np.argmin(scores))]
+        # ties within float round-off may resolve either way
+        if abs(np.sort(scores)[1] - scores.min()) > 1e-4 if len(cand) > 1 else True:
+            assert learned[b] == best, (b, learned[b], best)
