@@ -30,6 +30,9 @@ def main():
     args = ap.parse_args()
     torch.cuda.set_device(0)
     lib = gk.load()
+    if args.sched == "learned":
+        from graphkokkos_b200 import sched
+        sched.load_model()
     A = gk.gen_rmat(args.scale, 16, seed=args.seed, device="cuda")
     L = gk.extract_lower(A)
     del A
