@@ -79,7 +79,8 @@ GK_ACCUM_HASH = 3
 SIGNATURES = {
     "gk_mxmm_masked": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 3 + [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP]),
     "gk_tc_count": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
-    "gk_tc_count_variant": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, VP]),
+    "gk_tc_count_noalloc": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
+    "gk_tc_count_variant":(ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, VP]),
     "gk_mxmm_masked_variant": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 3 + [VP, ctypes.c_int, ctypes.c_int, VP]),
     "gk_tc_row_sums": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
     "gk_tc_count_batched": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, ctypes.c_int, VP]),

@@ -61,6 +61,17 @@ int Scratch::raw_alloc(void **p, size_t bytes) {
     if (n_ >= 64) return fail(GK_ERR_OOM, "internal: too many scratch allocations in one call");
     bytes = (bytes + 255) & ~size_t(255);
     if (bytes == 0) bytes = 256;
+    if (arena_) {
+        if (arena_used_ + bytes > arena_bytes_) {
+            char buf[160];
+            std::snprintf(buf, sizeof(buf), "fixed scratch exhausted: %zu bytes needed, %zu available",
+                          arena_used_ + bytes, arena_bytes_);
+            return fail(GK_ERR_OOM, buf);
+        }
+        *p = arena_ + arena_used_;
+        arena_used_ += bytes;
+        return GK_OK;
+    }
     cudaError_t e = cudaMallocAsync(p, bytes, stream_);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -51,6 +51,11 @@ Context &ctx();
 class Scratch {
 public:
     explicit Scratch(cudaStream_t s) : stream_(s) {}
+    // Bump allocation inside caller-provided device memory [arena, arena+bytes)
+    // instead of cudaMallocAsync; nothing is freed.  Used by the allocation-free
+    // entry point (noalloc.cu).
+    Scratch(cudaStream_t s, void *arena, size_t bytes)
+        : stream_(s), arena_(static_cast<char *>(arena)), arena_bytes_(bytes) {}
     ~Scratch() { release(); }
     Scratch(const Scratch &) = delete;
     Scratch &operator=(const Scratch &) = delete;
@@ -69,6 +74,8 @@ private:
     cudaStream_t stream_;
     void *ptrs_[64] = {};
     int n_ = 0;
+    char *arena_ = nullptr;
+    size_t arena_bytes_ = 0, arena_used_ = 0;
 };
 
 // Host-or-device staging of a CSR: if the arrays are host memory they are

@@ -102,6 +102,17 @@ int gk_mxmm_masked(const gk_csr *A, const gk_csr *B, const gk_csr *M, int32_t *C
  * *count receives the uint64 total (the reference returns int64). */
 int gk_tc_count(const gk_csr *L, uint64_t *count, int sched, void *stream);
 
+/* Same count as gk_tc_count, for callers that cannot have the library allocate
+ * GPU memory during the call (a process whose framework already reserved the
+ * device's memory, or a host that forbids allocations in its processing loop).
+ * No counterpart in the reference.  All scratch comes from one fixed 36 MiB
+ * device array that this library holds on every GPU it is loaded on; L may
+ * have at most 1,048,576 rows (GK_ERR_ARG beyond) and must be in device memory;
+ * *count may be host or device memory.  The first call on a device looks up the
+ * array's address, so make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race. */
+int gk_tc_count_noalloc(const gk_csr *L, uint64_t *count, int sched, void *stream);
+
 /* Per-vertex sums of C<L> = L·L: row_sums[i] = sum_j C(i,j), the number of
  * triangles whose largest vertex is i (a fused-epilogue variant of
  * triangle_counting_vertex, src/main.cpp:16-39). */
