@@ -5,6 +5,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Resident threads per SM the engine kernels are register-capped for
+// (launch bounds NT, GK_LB_THREADS / NT).
+#ifndef GK_LB_THREADS
+#define GK_LB_THREADS 1536
+#endif
+
 namespace gk {
 
 constexpr int EMPTY_KEY = -1;

@@ -14,7 +14,7 @@
 #pragma once
 
 template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT, (1536 / NT) < 1 ? 1 : (1536 / NT)) k_block(KArgs p) {
+__global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THREADS / NT)) k_block(KArgs p) {
     constexpr bool ACC = (EPI == EPI_WRITE);
     constexpr int NW = NT / 32;
     constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;  // MSA: CAP = log2 window width

@@ -48,18 +48,20 @@ struct Variant {
 
 constexpr int NV = 13;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
-// Hash tables run at load factor <= 1/4 (chunk <= cap/4) except variant 10.
+// Hash tables without a filter run at load factor <= 1/4 (chunk <= cap/4);
+// behind a filter of about 64 bits per mask entry only filter candidates
+// reach the table, and the large tables of variants 6-8 run at load <= 1/2.
 // columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum
 #define GK_VARIANT_TABLE { \
     {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3},   \
     {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3},   \
-    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 11, 1, 3},   \
-    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 11, 8, 3},   \
-    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 12, 4, 3},   \
-    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 12, 4, 3},   \
-    {K_HASH_BLOCK, 128, 32,  4096,  4096,  1024,  1024,  18, 14, 2, 3},   \
-    {K_HASH_BLOCK, 256, 32, 16384, 16384,  4096,  4096,  19, 16, 1, 3},   \
-    {K_HASH_BLOCK, 512, 32, 32768, 16384,  8192,  4096,  20, 17, 1, 3},   \
+    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 13, 1, 3},   \
+    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3},   \
+    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
+    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  4096,  1024,  1024,  18, 16, 2, 3},   \
+    {K_HASH_BLOCK, 256, 32,  8192, 16384,  4096,  4096,  19, 17, 1, 3},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  4096,  20, 18, 1, 3},   \
     {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2},   \
     {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2},   \
     {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1},   \

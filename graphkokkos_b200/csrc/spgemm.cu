@@ -266,6 +266,22 @@ __device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, i
     }
 }
 
+// Exact lookups of the filter candidates among the eight elements of x, y
+// (bit e of m set = element e passed the filter).  Each lane walks only its
+// own set bits, so a warp iterates as often as its busiest lane has
+// candidates instead of once per element position with a lane or two active.
+template <int CAP, bool ACC>
+__device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int4 &y, uint32_t av,
+                                            const int *keys, int *acc, unsigned &cnt) {
+    while (m) {
+        const int e = __ffs(m) - 1;
+        m &= m - 1;
+        const int lo = (e & 1) ? ((e & 4) ? y.y : x.y) : ((e & 4) ? y.x : x.x);
+        const int hi = (e & 1) ? ((e & 4) ? y.w : x.w) : ((e & 4) ? y.z : x.z);
+        exact_hash<CAP, ACC>((e & 2) ? hi : lo, av, keys, acc, cnt);
+    }
+}
+
 // The SUB lanes of a sub-group stream B[b0, b1): 16-byte vector loads, two in
 // flight per lane, scalar head/tail; with values, scalar loads of col and val.
 // With a filter, the eight elements of two vectors are tested against the
@@ -290,25 +306,13 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
                                    (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3) |
                                    (cand_bit<FLOG>(y.x, filt) << 4) | (cand_bit<FLOG>(y.y, filt) << 5) |
                                    (cand_bit<FLOG>(y.z, filt) << 6) | (cand_bit<FLOG>(y.w, filt) << 7);
-                if (m) {
-                    if (m & 1u) exact_hash<CAP, ACC>(x.x, av, keys, acc, cnt);
-                    if (m & 2u) exact_hash<CAP, ACC>(x.y, av, keys, acc, cnt);
-                    if (m & 4u) exact_hash<CAP, ACC>(x.z, av, keys, acc, cnt);
-                    if (m & 8u) exact_hash<CAP, ACC>(x.w, av, keys, acc, cnt);
-                    if (m & 16u) exact_hash<CAP, ACC>(y.x, av, keys, acc, cnt);
-                    if (m & 32u) exact_hash<CAP, ACC>(y.y, av, keys, acc, cnt);
-                    if (m & 64u) exact_hash<CAP, ACC>(y.z, av, keys, acc, cnt);
-                    if (m & 128u) exact_hash<CAP, ACC>(y.w, av, keys, acc, cnt);
-                }
+                exact_cands<CAP, ACC>(m, x, y, av, keys, acc, cnt);
             }
             if (q < n4) {
                 const int4 x = __ldg(base + q);
                 const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
                                    (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3);
-                if (m & 1u) exact_hash<CAP, ACC>(x.x, av, keys, acc, cnt);
-                if (m & 2u) exact_hash<CAP, ACC>(x.y, av, keys, acc, cnt);
-                if (m & 4u) exact_hash<CAP, ACC>(x.z, av, keys, acc, cnt);
-                if (m & 8u) exact_hash<CAP, ACC>(x.w, av, keys, acc, cnt);
+                exact_cands<CAP, ACC>(m, x, x, av, keys, acc, cnt);
             }
             int64_t tl = (b1 >> 2) << 2;
             if (tl < h1) tl = h1;
@@ -408,7 +412,7 @@ __device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, in
 // takes its next row from a global counter, so groups never wait on each
 // other for work.
 template <int G, int SUB, int NT, int CAP, int CHUNK, bool MCA, int FLOG, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT, 1536 / NT) k_group(KArgs p) {
+__global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
     constexpr int NG = NT / G;
     constexpr int S = G / SUB;
     constexpr bool ACC = (EPI == EPI_WRITE);
