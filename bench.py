@@ -273,45 +273,217 @@ def run_tc(args, wl, torch, gk, dist, rank, world):
     return line
 
 
+def ktruss_roofline(gk, torch, A, k, sched, peak, peak_kind):
+    """Per-variant CUDA-event durations and work of one profiled k-truss run
+    (every pass's support SpGEMM); the dominant variant's algorithmic bytes
+    over its summed launch time, and the whole loop's bytes over its time."""
+    lib = gk.load()
+    lib.gk_prof_enable(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, iters = gk.ktruss(A, k, sched=sched)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    rec = gk._lib.GkProfRec()
+    per = {}
+    for i in range(lib.gk_prof_count()):
+        lib.gk_prof_get(i, ctypes.byref(rec))
+        if not rec.rows:
+            continue
+        d = per.setdefault(rec.variant, dict(ms=0.0, work=0, a=0, m=0, rows=0, launches=0))
+        d["ms"] += rec.ms
+        d["work"] += rec.sum_work
+        d["a"] += rec.sum_a
+        d["m"] += rec.sum_m
+        d["rows"] += rec.rows
+        d["launches"] += 1
+    lib.gk_prof_enable(0)
+    for d in per.values():
+        # B-row column stream 4·W, A entries 4 B + two row pointers each,
+        # row pointers per row, and the support value written per mask entry
+        d["bytes"] = 4 * d["work"] + 20 * d["a"] + 16 * d["rows"] + 4 * d["m"]
+    dom = max(per, key=lambda v: per[v]["ms"])
+    d = per[dom]
+    achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
+    return {"kernel": f"masked SpGEMM variant {dom} (support S<C>=C·C, all passes)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "launch_ms": round(d["ms"] / d["launches"], 3),
+            "bytes_per_launch": d["bytes"] // d["launches"], "passes": iters,
+            "spgemm_bytes_total": sum(x["bytes"] for x in per.values()),
+            "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "launches": x["launches"]}
+                         for v, x in sorted(per.items())},
+            "profiled_wall_ms": round(wall * 1e3, 1)}
+
+
 def run_ktruss(args, wl, torch, gk, dist, rank, world):
     A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
-    iters = [0]
+    have_model = load_model(gk)
+    scheds = ["plain"] + (["learned"] if have_model else [])
+    lib = gk.load()
+    res = {}
+    ref = None
+    for sched in scheds:
+        state = {}
 
-    def fn():
-        T, it = gk.ktruss(A, wl["k"])
-        iters[0] = it
-    ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+        def fn():
+            T, it = gk.ktruss(A, wl["k"], sched=sched)
+            state["T"], state["it"] = T, it
+        if sched == scheds[-1]:
+            clocks = ClockSampler(torch.cuda.current_device())
+            clocks.start()
+            l0 = lib.gk_launch_count()
+        ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+        if sched == scheds[-1]:
+            launches = (lib.gk_launch_count() - l0) // (args.steps + args.warmup)
+            clk = clocks.stop()
+        T = state["T"]
+        sig = (state["it"], T.nnz, int(T.col.sum().item()))
+        assert ref is None or sig == ref, "schedulers disagree"
+        ref = sig
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res[sched] = {"value": (A.nnz // 2) * world / (ms_max / 1e3), "ms_per_step": ms_max}
+    head = scheds[-1]
     edges = A.nnz // 2
-    return {"metric": METRIC, "value": edges * world / (ms / 1e3), "unit": "edges/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic: seeded RMAT",
+    line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: seeded RMAT (a,b,c,d=.57,.19,.19,.05, edge factor 16), generated on the device",
             "config": {"workload": f"k-truss k={wl['k']} on RMAT-{wl['scale']} seed {wl['seed']}",
-                       "iterations": iters[0], "edges": edges}}
+                       "iterations": ref[0], "edges": edges, "truss_nnz": ref[1], "sched": head,
+                       "loop": "one CUDA graph per call (conditional while node around a captured pass)",
+                       "l2": "inputs larger than L2 (support SpGEMM streams > 100 GB per pass)"},
+            "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        line["roofline"] = ktruss_roofline(gk, torch, A, wl["k"], head, peak, peak_kind)
+        # end to end through the public API with pinned host CSR arrays
+        Ah = A.to("cpu")
+        Ah.rowptr = Ah.rowptr.pin_memory()
+        Ah.col = Ah.col.pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        T, it = gk.ktruss(Ah, wl["k"], sched=head)
+        e2e_s = time.perf_counter() - t0
+        assert (it, T.nnz) == ref[:2]
+        line["e2e"] = {"value": edges / e2e_s, "unit": "edges/s", "ms_per_step": e2e_s * 1e3,
+                       "h2d_bytes_per_step": 8 * (A.m + 1) + 4 * A.nnz,
+                       "d2h_bytes_per_step": 8 * (A.m + 1) + 4 * T.nnz,
+                       "api": "gk_ktruss with pinned host CSR arrays (result written back to them)"}
+    return line
 
 
-def run_bc(args, wl, torch, gk, dist, rank, world):
-    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
-    rng = np.random.default_rng(wl["src_seed"])
-    src = rng.choice(A.m, size=wl["nsrc"], replace=False)
-    out = [None]
-
-    def fn():
-        out[0] = gk.bc_batch(A, src)
-    ms = time_steps(torch, fn, args.steps, args.warmup, dist)
-    # TEPS: undirected edges in each source's component
+def bc_traversed(A, src):
+    """Undirected edges in each source's component, summed over the sources
+    (the TEPS numerator), and the directed edges of those components."""
     import scipy.sparse as sp
     import scipy.sparse.csgraph as cg
     rp = A.rowptr.cpu().numpy()
     col = A.col.cpu().numpy()
     M = sp.csr_matrix((np.ones(len(col), dtype=np.int8), col, rp), shape=(A.m, A.m))
     ncomp, lab = cg.connected_components(M, directed=False)
-    edges_per_comp = np.bincount(lab[np.repeat(np.arange(A.m), np.diff(rp))], minlength=ncomp) // 2
-    traversed = int(edges_per_comp[lab[src]].sum())
-    return {"metric": METRIC, "value": traversed * world / (ms / 1e3), "unit": "TEPS", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded RMAT",
+    directed_per_comp = np.bincount(lab[np.repeat(np.arange(A.m), np.diff(rp))], minlength=ncomp)
+    return int((directed_per_comp[lab[src]] // 2).sum()), int(directed_per_comp[lab[src]].sum())
+
+
+def bc_cpu_baseline(A, nsample=8, seed=7):
+    """The reference's betweenness_centrality_batch (oracle/_ref via the
+    Kokkos-API shim; sources 0..b-1 after relabelling) on a bounded source
+    sample, single-threaded (its row split is unsafe with more threads)."""
+    import oracle
+    if not oracle.ref_available():
+        return None
+    Ah = A.numpy()
+    src = np.random.default_rng(seed).choice(A.m, size=nsample, replace=False)
+    R, _ = oracle.relabel_sources_first(Ah, src)
+    t0 = time.perf_counter()
+    oracle.ref_bc_float(R, nsample, threads=1)
+    sec = time.perf_counter() - t0
+    trav, _ = bc_traversed(A, src)
+    return {"value": trav / sec, "unit": "TEPS", "cores": 1, "kind": "reference",
+            "sample": f"{nsample} sources (seed {seed}) of the same graph, {sec:.1f} s, "
+                      "reference BC (float, int32 path counts), one thread"}
+
+
+def run_bc(args, wl, torch, gk, dist, rank, world):
+    from graphkokkos_b200 import sched as gsched
+    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
+    rng = np.random.default_rng(wl["src_seed"])
+    src = rng.choice(A.m, size=wl["nsrc"], replace=False)
+    lib = gk.load()
+    scheds = ["plain"]
+    if os.path.exists(gsched.BC_MODEL_PATH):
+        gsched.load_bc_model()
+        scheds.append("learned")
+    traversed, directed = bc_traversed(A, src)
+    res = {}
+    ref = None
+    for sched in scheds:
+        out = [None]
+
+        def fn():
+            out[0] = gk.bc_batch(A, src, sched=sched)
+        if sched == scheds[-1]:
+            clocks = ClockSampler(torch.cuda.current_device())
+            clocks.start()
+            l0 = lib.gk_launch_count()
+        ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+        if sched == scheds[-1]:
+            launches = (lib.gk_launch_count() - l0) // (args.steps + args.warmup)
+            clk = clocks.stop()
+        got = out[0].cpu().numpy()
+        if ref is None:
+            ref = got
+        else:
+            assert np.allclose(got, ref, rtol=1e-12, atol=1e-9), "schedulers disagree"
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res[sched] = {"value": traversed * world / (ms_max / 1e3), "ms_per_step": ms_max}
+    head = scheds[-1]
+    line = {"metric": METRIC, "value": res[head]["value"], "unit": "TEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded RMAT (a,b,c,d=.57,.19,.19,.05, edge factor 16), generated on the device; "
+                    f"{wl['nsrc']} sources sampled uniformly (seed {wl['src_seed']})",
             "config": {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources",
-                       "teps_all_edges": (A.nnz // 2) * len(src) / (ms / 1e3)}}
+                       "vertices": A.m, "nnz": A.nnz, "sched": head,
+                       "teps_numerator": "undirected edges in each source's component, summed over sources",
+                       "teps_all_edges": (A.nnz // 2) * len(src) / (res[head]["ms_per_step"] / 1e3),
+                       "loop": "forward and backward levels as CUDA graphs (conditional while nodes)",
+                       "l2": f"sigma and R arrays of {2 * A.m * 512 * 8 / 1e9:.1f} GB exceed L2"},
+            "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        # algorithmic bytes: 8 B of sigma per (directed edge, source) in the
+        # forward sweep, 16 B of sigma and R in the backward sweep, plus the
+        # FP64 sigma, R writes and the final read per (vertex, source)
+        alg = 24 * directed + 24 * A.m * len(src)
+        ach = alg / (res[head]["ms_per_step"] / 1e3) / 1e9
+        line["roofline"] = {"kernel": "batched BC, all levels of one step", "bound": "hbm", "achieved": round(ach, 1),
+                            "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4),
+                            "traffic": None, "bytes_per_step": alg}
+        # end to end through the public API: host CSR (pinned), host sources, host result
+        Ah = A.to("cpu")
+        Ah.rowptr = Ah.rowptr.pin_memory()
+        Ah.col = Ah.col.pin_memory()
+        gk.bc_batch(Ah, src, sched=head)
+        torch.cuda.synchronize()
+        e2e_steps = max(1, min(args.steps, 3))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            bh = gk.bc_batch(Ah, src, sched=head)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        assert np.allclose(np.asarray(bh), ref, rtol=1e-12, atol=1e-9)
+        line["e2e"] = {"value": traversed / e2e_s, "unit": "TEPS", "ms_per_step": e2e_s * 1e3,
+                       "h2d_bytes_per_step": 8 * (A.m + 1) + 4 * A.nnz + 4 * len(src),
+                       "d2h_bytes_per_step": 8 * A.m, "api": "gk_bc_batch with pinned host CSR arrays"}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = bc_cpu_baseline(A)
+    return line
 
 
 def main_ours(args):

@@ -109,6 +109,10 @@ SIGNATURES = {
     "gk_mlp_loss_grad": (ctypes.c_int, [VP, VP, VP, VP, ctypes.c_int, VP, VP, VP]),
     "gk_mlp_train": (ctypes.c_int, [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_float, VP, VP]),
     "gk_mlp_forward": (ctypes.c_int, [VP, VP, ctypes.c_int, VP, VP]),
+    "gk_bc_set_model": (ctypes.c_int, [VP, ctypes.c_size_t]),
+    "gk_bc_has_model": (ctypes.c_int, []),
+    "gk_bc_tune": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, ctypes.c_int, VP, VP, VP, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_int), VP]),
     "gk_prof_enable": (ctypes.c_int, [ctypes.c_int]),
     "gk_prof_count": (ctypes.c_int, []),
     "gk_prof_flush": (ctypes.c_int, []),

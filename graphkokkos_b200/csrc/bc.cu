@@ -14,16 +14,34 @@
 //                                bytes contiguous (4 KB at W = 512)
 //   level bitmaps F_d[v*T + t]   bit l of word t <=> source 32t+l is at depth d
 //   visited bitmap V[v*T + t]
-// One warp owns one vertex; lane l owns sources {32t + l}.  A neighbour is
-// skipped after one broadcast load of its T bitmap words unless it carries a
-// frontier bit this vertex still needs, so sigma/R are only read where the
-// algebra has a term.  Vertices with more than HEAVY neighbours are processed
-// by a whole CTA (warps split the neighbour list, partial sums reduced in
-// shared memory).  R(v,s) = (1+delta)/sigma replaces the reference's
-// Nspinv∘Bcu; delta is summed into bc[v] as soon as it is final.
+// Forward levels run one of two kernel shapes, chosen per level on the device:
+//   pull  one warp per vertex with sources still open: its lanes test 32
+//         in-neighbours' frontier words at a time, then for each neighbour that
+//         carries a needed bit the lanes (one per source) add sigma;
+//   push  one warp per frontier vertex: its lanes test 32 out-neighbours'
+//         visited words at a time, then add sigma into the new vertices with
+//         FP64 atomics.  sigma are path counts, integers below 2^53 in FP64, so
+//         the order of the additions does not change them.
+// The plain rule picks push while the frontier's edges are few against the
+// edges still to explore (Beamer's direction-optimising rule); the learned
+// rule is an MLP over the level's frontier statistics, trained on measured
+// per-level times of both shapes.  Backward levels pull: one warp per vertex
+// of level d, lanes testing 32 successors' level-(d+1) words at a time.
+// Vertices with more than BC_HEAVY neighbours are handled by a whole CTA.
+// R(v,s) = (1+delta)/sigma replaces the reference's Nspinv∘Bcu; delta is summed
+// into bc[v] as soon as it is final, in a fixed order (deterministic).
+//
+// Every kernel reads the level index and the level bitmaps from device state,
+// so the level loops are CUDA graphs: a conditional while node around one
+// captured level, the condition set by the level's last kernel.  Both forward
+// shapes are launched every level and the one not chosen returns at once.
+#include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "gk_common.cuh"
+#include "gk_device.cuh"
+#include "gk_sched.cuh"
 
 namespace gk {
 
@@ -31,6 +49,31 @@ int transpose_device(const DevCsr &A, int64_t *orp, int32_t *ocol, int32_t *oval
 
 constexpr int BC_HEAVY = 512;
 constexpr int BC_NW_HEAVY = 8;  // T=16: 8*16*32 doubles = 32 KB of static shared memory
+constexpr int BC_PULL = 0, BC_PUSH = 1;
+constexpr int BC_LEVEL_BATCH = 16;  // level bitmaps allocated at a time
+constexpr int BC_FEAT = NFEAT;
+
+// learned forward-shape model (same network as the row-bin scheduler's;
+// outputs 0 and 1 predict log2 microseconds of a pull and a push level)
+__device__ float d_mlp_bc[MLP_SIZE];
+static std::mutex g_bc_model_mutex;
+static std::vector<float> g_bc_model;
+static int g_bc_model_version = 0;
+static int g_bc_uploaded[64];
+
+struct BcState {
+    uint32_t **fptr;               // fptr[d] = F_d (m x T words), d = 1..levels
+    int d;                         // forward: deepest level built so far
+    int levels;                    // bitmaps allocated
+    int bd;                        // backward: level being processed
+    int mode;                      // forward shape of the current level
+    int done;                      // forward finished (next frontier empty)
+    int pad;
+    unsigned long long nf, ef, bf;  // F_d: vertices, their out-edges, (vertex, source) pairs
+    unsigned long long nn, en, bn;  // F_{d+1} under construction
+    unsigned long long visited;     // (vertex, source) pairs reached, sources included
+    unsigned long long pushes, pulls;
+};
 
 template <int T>
 __device__ __forceinline__ void load_words(const uint32_t *p, uint32_t (&w)[T]) {
@@ -47,6 +90,25 @@ __device__ __forceinline__ void load_words(const uint32_t *p, uint32_t (&w)[T]) 
 #pragma unroll
         for (int t = 0; t < T; ++t) w[t] = __ldg(p + t);
     }
+}
+
+// plain (coherent) loads, for words other CTAs of the same kernel may change
+template <int T>
+__device__ __forceinline__ void load_words_rw(const uint32_t *p, uint32_t (&w)[T]) {
+#pragma unroll
+    for (int t = 0; t < T; ++t) w[t] = p[t];
+}
+
+// One atomic per block and counter.
+__device__ __forceinline__ void add_level_stats(unsigned long long n, unsigned long long e, unsigned long long b,
+                                                unsigned long long *dst) {
+    __shared__ unsigned long long red[32];
+    n = block_sum(n, red);
+    if (threadIdx.x == 0 && n) atomicAdd(dst, n);
+    e = block_sum(e, red);
+    if (threadIdx.x == 0 && e) atomicAdd(dst + 1, e);
+    b = block_sum(b, red);
+    if (threadIdx.x == 0 && b) atomicAdd(dst + 2, b);
 }
 
 __global__ void k_bc_seed(DevCsr A, const int32_t *src, int nsrc, int T, int W, uint32_t *F1, uint32_t *V,
@@ -69,57 +131,148 @@ __global__ void k_bc_seed(DevCsr A, const int32_t *src, int nsrc, int T, int W, 
     }
 }
 
-// forward pull for one vertex by one warp (or one warp's share of the neighbours)
+// Statistics of F_1 (thread per vertex) into st->nf/ef/bf.
 template <int T>
-__device__ __forceinline__ bool fwd_accumulate(const DevCsr &AT, int64_t e0, int64_t e1, int64_t estride,
-                                               const uint32_t *__restrict__ Fd, const uint32_t (&need)[T],
-                                               const double *__restrict__ sigma, int W, int lane,
-                                               double (&acc)[T]) {
-    bool any = false;
-    for (int64_t e = e0; e < e1; e += estride) {
-        const int k = __ldg(AT.col + e);
+__global__ void k_bc_first_stats(DevCsr A, const uint32_t *F1, BcState *st, int nsrc) {
+    unsigned long long n = 0, e = 0, b = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < A.m; v += stride) {
         uint32_t f[T];
-        load_words<T>(Fd + (int64_t)k * T, f);
-        uint32_t hit = 0;
+        load_words<T>(F1 + v * T, f);
+        int c = 0;
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-            f[t] &= need[t];
-            hit |= f[t];
+        for (int t = 0; t < T; ++t) c += __popc(f[t]);
+        if (c) {
+            ++n;
+            e += static_cast<unsigned long long>(A.rp[v + 1] - A.rp[v]);
+            b += c;
         }
-        if (!hit) continue;
-        any = true;
-        const double a = AT.val ? static_cast<double>(__ldg(AT.val + e)) : 1.0;
-        const double *__restrict__ sk = sigma + (int64_t)k * W + lane;
+    }
+    add_level_stats(n, e, b, &st->nf);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&st->visited, static_cast<unsigned long long>(nsrc));
+}
+
+// Features of the current level (inputs of the learned shape model).
+__device__ void bc_features(const BcState *st, int64_t m, int64_t nnz, int W, float *f) {
+    const double total = static_cast<double>(m) * W;
+    const double unvisited = total > st->visited ? total - static_cast<double>(st->visited) : 0.0;
+    const double mu = static_cast<double>(nnz) * unvisited / (total > 0 ? total : 1.0);  // edges left to explore
+    f[0] = static_cast<float>(log2(1.0 + st->nf));
+    f[1] = static_cast<float>(log2(1.0 + st->ef));
+    f[2] = static_cast<float>(log2(1.0 + st->bf));
+    f[3] = static_cast<float>(log2(1.0 + mu));
+    f[4] = static_cast<float>(log2(1.0 + m));
+    f[5] = static_cast<float>(log2(1.0 + nnz));
+    f[6] = static_cast<float>(log2(static_cast<double>(W)));
+    f[7] = static_cast<float>(st->d);
+}
+
+// Plain rule (Beamer's direction-optimising BFS, alpha = 14, beta = 24): push
+// while the frontier's out-edges are few against the edges left to explore,
+// or while the frontier holds few vertices.
+__device__ int bc_plain_shape(const BcState *st, int64_t m, int64_t nnz, int W) {
+    const double total = static_cast<double>(m) * W;
+    const double unvisited = total > st->visited ? total - static_cast<double>(st->visited) : 0.0;
+    const double mu = static_cast<double>(nnz) * unvisited / (total > 0 ? total : 1.0);
+    if (static_cast<double>(st->ef) * 14.0 < mu) return BC_PUSH;
+    if (static_cast<double>(st->nf) * 24.0 < static_cast<double>(m)) return BC_PUSH;
+    return BC_PULL;
+}
+
+// Picks the forward shape of level st->d (force >= 0 overrides) and logs the
+// level's features when feat_log is given.
+__global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_t nnz, int W, float *feat_log,
+                            int log_cap) {
+    float f[BC_FEAT];
+    bc_features(st, m, nnz, W, f);
+    int mode;
+    if (force >= 0) {
+        mode = force;
+    } else if (sched == GK_SCHED_LEARNED) {
+        float x[NFEAT], h1[MLP_H], h2[MLP_H], out[NV];
+        mlp_forward(d_mlp_bc, f, x, h1, h2, out);
+        mode = out[BC_PUSH] < out[BC_PULL] ? BC_PUSH : BC_PULL;
+    } else {
+        mode = bc_plain_shape(st, m, nnz, W);
+    }
+    st->mode = mode;
+    if (mode == BC_PUSH) ++st->pushes;
+    else ++st->pulls;
+    const int d = st->d;
+    if (feat_log && d >= 1 && d <= log_cap)
+        for (int i = 0; i < BC_FEAT; ++i) feat_log[(d - 1) * BC_FEAT + i] = f[i];
+}
+
+// ---------------------------------------------------------------------------
+// forward, pull: in-neighbours (AT) of a vertex with open sources
+// ---------------------------------------------------------------------------
+// Lanes test 32 neighbours' frontier words at a time; each neighbour carrying
+// a needed bit then has its sigma words added by the lanes of those sources.
+template <int T>
+__device__ __forceinline__ bool pull_sigma(const DevCsr &AT, int64_t ebeg, int64_t e1, int64_t estep,
+                                           const uint32_t *__restrict__ Fd, const uint32_t (&need)[T],
+                                           const double *__restrict__ sigma, int W, int lane, double (&acc)[T]) {
+    bool any = false;
+    for (int64_t base = ebeg; base < e1; base += estep) {
+        const int64_t e = base + lane;
+        int u = 0;
+        uint32_t hitw = 0;
+        if (e < e1) {
+            u = __ldg(AT.col + e);
+            uint32_t f[T];
+            load_words<T>(Fd + (int64_t)u * T, f);
 #pragma unroll
-        for (int t = 0; t < T; ++t)
-            if ((f[t] >> lane) & 1u) acc[t] += a * __ldg(sk + 32 * t);
+            for (int t = 0; t < T; ++t) hitw |= f[t] & need[t];
+        }
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, hitw != 0);
+        if (bal) any = true;
+        while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int uu = __shfl_sync(0xFFFFFFFFu, u, j);
+            const double a = AT.val ? static_cast<double>(__ldg(AT.val + base + j)) : 1.0;
+            uint32_t f[T];
+            load_words<T>(Fd + (int64_t)uu * T, f);
+            const double *__restrict__ su = sigma + (int64_t)uu * W + lane;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                const uint32_t bits = f[t] & need[t];
+                if (bits && ((bits >> lane) & 1u)) acc[t] += a * __ldg(su + 32 * t);
+            }
+        }
     }
     return any;
 }
 
+// New level bits, sigma and visited words of vertex i; returns the number of
+// new (vertex, source) pairs (valid in every lane).
 template <int T>
-__device__ __forceinline__ void fwd_emit(int64_t i, int W, int lane, const uint32_t (&vis)[T], const double (&acc)[T],
-                                         uint32_t *Fn, uint32_t *V, double *sigma, unsigned *progress) {
-    uint32_t anyb = 0;
+__device__ __forceinline__ int pull_emit(int64_t i, int W, int lane, const uint32_t (&vis)[T],
+                                         const double (&acc)[T], uint32_t *Fn, uint32_t *V, double *sigma) {
+    int c = 0;
 #pragma unroll
     for (int t = 0; t < T; ++t) {
         const uint32_t nb = __ballot_sync(0xFFFFFFFFu, acc[t] != 0.0);
-        anyb |= nb;
+        c += __popc(nb);
         if ((nb >> lane) & 1u) sigma[i * W + 32 * t + lane] = acc[t];
         if (lane == t) {
             Fn[i * T + t] = nb;
             V[i * T + t] = vis[t] | nb;
         }
     }
-    if (lane == 0 && anyb) atomicAdd(progress, 1u);
+    return c;
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) k_bc_forward(DevCsr AT, const uint32_t *__restrict__ Fd, uint32_t *Fn,
-                                                    uint32_t *V, double *sigma, int W, const uint32_t *act,
-                                                    unsigned *progress) {
+__global__ void __launch_bounds__(256) k_bc_pull(DevCsr AT, DevCsr A, BcState *st, uint32_t *V, double *sigma,
+                                                 int W, const uint32_t *act) {
+    if (st->mode != BC_PULL) return;
+    const int d = st->d;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    unsigned long long n = 0, e = 0, b = 0;
     for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < AT.m; i += warps) {
         const int64_t e0 = AT.rp[i], e1 = AT.rp[i + 1];
         if (e0 == e1 || e1 - e0 > BC_HEAVY) continue;
@@ -135,18 +288,28 @@ __global__ void __launch_bounds__(256) k_bc_forward(DevCsr AT, const uint32_t *_
         double acc[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
-        if (!fwd_accumulate<T>(AT, e0, e1, 1, Fd, need, sigma, W, lane, acc)) continue;
-        fwd_emit<T>(i, W, lane, vis, acc, Fn, V, sigma, progress);
+        if (!pull_sigma<T>(AT, e0, e1, 32, Fd, need, sigma, W, lane, acc)) continue;
+        const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
+        if (c && lane == 0) {
+            ++n;
+            e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
+            b += c;
+        }
     }
+    add_level_stats(n, e, b, &st->nn);
 }
 
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_forward_heavy(DevCsr AT, const int32_t *heavy, int nheavy,
-                                                                      const uint32_t *__restrict__ Fd, uint32_t *Fn,
-                                                                      uint32_t *V, double *sigma, int W,
-                                                                      const uint32_t *act, unsigned *progress) {
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_heavy(DevCsr AT, DevCsr A, const int32_t *heavy,
+                                                                    int nheavy, BcState *st, uint32_t *V,
+                                                                    double *sigma, int W, const uint32_t *act) {
+    if (st->mode != BC_PULL) return;
     __shared__ double part[BC_NW_HEAVY][T][32];
+    const int d = st->d;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long n = 0, e = 0, b = 0;
     for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int64_t i = heavy[h];
         const int64_t e0 = AT.rp[i], e1 = AT.rp[i + 1];
@@ -162,7 +325,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_forward_heavy(DevCsr AT
         double acc[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
-        fwd_accumulate<T>(AT, e0 + warp, e1, BC_NW_HEAVY, Fd, need, sigma, W, lane, acc);
+        pull_sigma<T>(AT, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fd, need, sigma, W, lane, acc);
 #pragma unroll
         for (int t = 0; t < T; ++t) part[warp][t][lane] = acc[t];
         __syncthreads();
@@ -173,15 +336,161 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_forward_heavy(DevCsr AT
                 for (int w = 0; w < BC_NW_HEAVY; ++w) sum += part[w][t][lane];
                 acc[t] = sum;
             }
-            fwd_emit<T>(i, W, lane, vis, acc, Fn, V, sigma, progress);
+            const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
+            if (c && lane == 0) {
+                ++n;
+                e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
+                b += c;
+            }
         }
         __syncthreads();
     }
+    add_level_stats(n, e, b, &st->nn);
 }
 
+// ---------------------------------------------------------------------------
+// forward, push: out-neighbours (A) of frontier vertices
+// ---------------------------------------------------------------------------
+// V is the visited state before this level (updated by k_bc_push_finish), so
+// every depth-d predecessor of a new vertex adds its sigma.
+template <int T>
+__device__ __forceinline__ void push_sigma(const DevCsr &A, int64_t ebeg, int64_t e1, int64_t estep,
+                                           const uint32_t (&fu)[T], const double (&su)[T],
+                                           const uint32_t *__restrict__ V, double *sigma, uint32_t *Fn, int W,
+                                           int T_, int lane) {
+    for (int64_t base = ebeg; base < e1; base += estep) {
+        const int64_t e = base + lane;
+        int v = 0;
+        uint32_t hitw = 0;
+        if (e < e1) {
+            v = __ldg(A.col + e);
+            uint32_t w[T];
+            load_words<T>(V + (int64_t)v * T, w);
+#pragma unroll
+            for (int t = 0; t < T; ++t) hitw |= fu[t] & ~w[t];
+        }
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, hitw != 0);
+        while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int vv = __shfl_sync(0xFFFFFFFFu, v, j);
+            const double a = A.val ? static_cast<double>(__ldg(A.val + base + j)) : 1.0;
+            uint32_t w[T];
+            load_words<T>(V + (int64_t)vv * T, w);
+            double *sv = sigma + (int64_t)vv * W + lane;
+            uint32_t mine = 0;
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                const uint32_t bits = fu[t] & ~w[t];
+                if (bits) {
+                    if ((bits >> lane) & 1u) atomicAdd(sv + 32 * t, a * su[t]);
+                    if (lane == t) mine = bits;
+                }
+            }
+            if (mine) atomicOr(Fn + (int64_t)vv * T_ + lane, mine);
+        }
+    }
+}
+
+template <int T>
+__device__ __forceinline__ bool push_source(int64_t u, const uint32_t *__restrict__ Fd, const double *sigma, int W,
+                                            int lane, uint32_t (&fu)[T], double (&su)[T]) {
+    load_words<T>(Fd + u * T, fu);
+    uint32_t any = 0;
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        any |= fu[t];
+        su[t] = ((fu[t] >> lane) & 1u) ? sigma[u * W + 32 * t + lane] : 0.0;
+    }
+    return any != 0;
+}
+
+template <int T>
+__global__ void __launch_bounds__(256) k_bc_push(DevCsr A, BcState *st, const uint32_t *V, double *sigma, int W) {
+    if (st->mode != BC_PUSH) return;
+    const int d = st->d;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    uint32_t *Fn = st->fptr[d + 1];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < A.m; u += warps) {
+        const int64_t e0 = A.rp[u], e1 = A.rp[u + 1];
+        if (e0 == e1 || e1 - e0 > BC_HEAVY) continue;
+        uint32_t fu[T];
+        double su[T];
+        if (!push_source<T>(u, Fd, sigma, W, lane, fu, su)) continue;
+        push_sigma<T>(A, e0, e1, 32, fu, su, V, sigma, Fn, W, T, lane);
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_push_heavy(DevCsr A, const int32_t *heavy, int nheavy,
+                                                                    BcState *st, const uint32_t *V, double *sigma,
+                                                                    int W) {
+    if (st->mode != BC_PUSH) return;
+    const int d = st->d;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    uint32_t *Fn = st->fptr[d + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
+        const int64_t u = heavy[h];
+        uint32_t fu[T];
+        double su[T];
+        if (!push_source<T>(u, Fd, sigma, W, lane, fu, su)) continue;
+        push_sigma<T>(A, A.rp[u] + 32 * warp, A.rp[u + 1], 32 * BC_NW_HEAVY, fu, su, V, sigma, Fn, W, T, lane);
+    }
+}
+
+// After a push level: V |= F_{d+1} and the statistics of F_{d+1}.
+template <int T>
+__global__ void k_bc_push_finish(DevCsr A, BcState *st, uint32_t *V) {
+    if (st->mode != BC_PUSH) return;
+    const uint32_t *__restrict__ Fn = st->fptr[st->d + 1];
+    unsigned long long n = 0, e = 0, b = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < A.m; v += stride) {
+        uint32_t f[T];
+        load_words_rw<T>(Fn + v * T, f);
+        int c = 0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) c += __popc(f[t]);
+        if (c) {
+#pragma unroll
+            for (int t = 0; t < T; ++t) V[v * T + t] |= f[t];
+            ++n;
+            e += static_cast<unsigned long long>(A.rp[v + 1] - A.rp[v]);
+            b += c;
+        }
+    }
+    add_level_stats(n, e, b, &st->nn);
+}
+
+// End of a forward level: an empty F_{d+1} ends the sweep (F_1..F_d are the
+// BFS layers); otherwise F_{d+1} becomes the frontier.  Inside the graph the
+// loop continues while a bitmap for the next level is allocated.
+__global__ void k_bc_fwd_end(BcState *st, int64_t max_depth, cudaGraphConditionalHandle h, int in_graph) {
+    int more = 0;
+    if (st->nn == 0) {
+        st->done = 1;
+    } else {
+        st->visited += st->bn;
+        st->nf = st->nn;
+        st->ef = st->en;
+        st->bf = st->bn;
+        st->d += 1;
+        more = (st->d + 1 <= st->levels && st->d < max_depth) ? 1 : 0;
+    }
+    st->nn = st->en = st->bn = 0;
+    if (in_graph) cudaGraphSetConditional(h, static_cast<unsigned>(more));
+}
+
+// ---------------------------------------------------------------------------
+// backward: R = (1 + delta) / sigma from level D up to level 1
+// ---------------------------------------------------------------------------
 // deepest level: R = 1/sigma (Bcu = 1 there)
 template <int T>
-__global__ void k_bc_rinit(int64_t m, const uint32_t *__restrict__ Fd, const double *sigma, double *R, int W) {
+__global__ void k_bc_rinit(int64_t m, const BcState *st, const double *sigma, double *R, int W) {
+    const uint32_t *__restrict__ Fd = st->fptr[st->d];
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < m; v += warps) {
@@ -194,25 +503,35 @@ __global__ void k_bc_rinit(int64_t m, const uint32_t *__restrict__ Fd, const dou
 }
 
 template <int T>
-__device__ __forceinline__ void bwd_accumulate(const DevCsr &A, int64_t e0, int64_t e1, int64_t estride,
-                                               const uint32_t *__restrict__ Fn, const uint32_t (&fv)[T],
-                                               const double *__restrict__ R, int W, int lane, double (&sum)[T]) {
-    for (int64_t e = e0; e < e1; e += estride) {
-        const int w = __ldg(A.col + e);
-        uint32_t f[T];
-        load_words<T>(Fn + (int64_t)w * T, f);
-        uint32_t hit = 0;
+__device__ __forceinline__ void pull_r(const DevCsr &A, int64_t ebeg, int64_t e1, int64_t estep,
+                                       const uint32_t *__restrict__ Fn, const uint32_t (&fv)[T],
+                                       const double *__restrict__ R, int W, int lane, double (&sum)[T]) {
+    for (int64_t base = ebeg; base < e1; base += estep) {
+        const int64_t e = base + lane;
+        int w = 0;
+        uint32_t hitw = 0;
+        if (e < e1) {
+            w = __ldg(A.col + e);
+            uint32_t f[T];
+            load_words<T>(Fn + (int64_t)w * T, f);
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-            f[t] &= fv[t];
-            hit |= f[t];
+            for (int t = 0; t < T; ++t) hitw |= f[t] & fv[t];
         }
-        if (!hit) continue;
-        const double a = A.val ? static_cast<double>(__ldg(A.val + e)) : 1.0;
-        const double *__restrict__ rw = R + (int64_t)w * W + lane;
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, hitw != 0);
+        while (bal) {
+            const int j = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int ww = __shfl_sync(0xFFFFFFFFu, w, j);
+            const double a = A.val ? static_cast<double>(__ldg(A.val + base + j)) : 1.0;
+            uint32_t f[T];
+            load_words<T>(Fn + (int64_t)ww * T, f);
+            const double *__restrict__ rw = R + (int64_t)ww * W + lane;
 #pragma unroll
-        for (int t = 0; t < T; ++t)
-            if ((f[t] >> lane) & 1u) sum[t] += a * __ldg(rw + 32 * t);
+            for (int t = 0; t < T; ++t) {
+                const uint32_t bits = f[t] & fv[t];
+                if (bits && ((bits >> lane) & 1u)) sum[t] += a * __ldg(rw + 32 * t);
+            }
+        }
     }
 }
 
@@ -236,9 +555,11 @@ __device__ __forceinline__ void bwd_emit(int64_t v, int W, int lane, const uint3
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) k_bc_backward(DevCsr A, const uint32_t *__restrict__ Fd,
-                                                     const uint32_t *__restrict__ Fn, const double *sigma, double *R,
+__global__ void __launch_bounds__(256) k_bc_backward(DevCsr A, const BcState *st, const double *sigma, double *R,
                                                      int W, double *bc) {
+    const int d = st->bd;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < A.m; v += warps) {
@@ -253,18 +574,19 @@ __global__ void __launch_bounds__(256) k_bc_backward(DevCsr A, const uint32_t *_
         double sum[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
-        bwd_accumulate<T>(A, e0, e1, 1, Fn, fv, R, W, lane, sum);
+        pull_r<T>(A, e0, e1, 32, Fn, fv, R, W, lane, sum);
         bwd_emit<T>(v, W, lane, fv, sum, sigma, R, bc);
     }
 }
 
 template <int T>
 __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_heavy(DevCsr A, const int32_t *heavy, int nheavy,
-                                                                       const uint32_t *__restrict__ Fd,
-                                                                       const uint32_t *__restrict__ Fn,
-                                                                       const double *sigma, double *R, int W,
-                                                                       double *bc) {
+                                                                       const BcState *st, const double *sigma,
+                                                                       double *R, int W, double *bc) {
     __shared__ double part[BC_NW_HEAVY][T][32];
+    const int d = st->bd;
+    const uint32_t *__restrict__ Fd = st->fptr[d];
+    const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
         const int64_t v = heavy[h];
@@ -277,7 +599,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_heavy(DevCsr A
         double sum[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
-        bwd_accumulate<T>(A, A.rp[v] + warp, A.rp[v + 1], BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
+        pull_r<T>(A, A.rp[v] + 32 * warp, A.rp[v + 1], 32 * BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
 #pragma unroll
         for (int t = 0; t < T; ++t) part[warp][t][lane] = sum[t];
         __syncthreads();
@@ -294,6 +616,11 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_heavy(DevCsr A
     }
 }
 
+__global__ void k_bc_bwd_end(BcState *st, cudaGraphConditionalHandle h, int in_graph) {
+    st->bd -= 1;
+    if (in_graph) cudaGraphSetConditional(h, st->bd >= 1 ? 1u : 0u);
+}
+
 __global__ void k_heavy_list(DevCsr A, int32_t *list, int *count) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.m; i += stride)
@@ -301,27 +628,106 @@ __global__ void k_heavy_list(DevCsr A, int32_t *list, int *count) {
 }
 
 // ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
 struct BcBuffers {
     DevCsr A, AT;
     int32_t *heavyA, *heavyAT;
     int nheavyA, nheavyAT;
 };
 
+// Options of a BC run: scheduler, a forced forward shape (autotuning), and
+// per-level logs of the forward levels (host arrays, may be null).
+struct BcOptions {
+    int sched = GK_SCHED_PLAIN;
+    int force = -1;
+    bool host_loop = false;  // drive the levels from the host (always with logging)
+    float *level_ms = nullptr;
+    float *level_feat = nullptr;
+    int *level_mode = nullptr;
+    int log_cap = 0;
+    int *levels_out = nullptr;
+};
+
+// A captured level loop: a graph with one conditional while node.
+class LevelGraph {
+public:
+    ~LevelGraph() {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (g_) cudaGraphDestroy(g_);
+        if (cs_) cudaStreamDestroy(cs_);
+    }
+    // Starts capturing the loop body; returns false where conditional graphs
+    // are unavailable.
+    bool begin(cudaGraphConditionalHandle *h) {
+        if (cudaGraphCreate(&g_, 0) != cudaSuccess) return false;
+        if (cudaGraphConditionalHandleCreate(h, g_, 1, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = *h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g_, nullptr, 0, &np) != cudaSuccess) return false;
+        if (cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking) != cudaSuccess) return false;
+        if (cudaStreamBeginCaptureToGraph(cs_, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return false;
+        capturing_ = true;
+        return true;
+    }
+    cudaStream_t stream() const { return cs_; }
+    int end() {
+        cudaGraph_t body = nullptr;
+        capturing_ = false;
+        cudaError_t e = cudaStreamEndCapture(cs_, &body);
+        if (e != cudaSuccess) return cuda_fail(e, "BC level capture");
+        e = cudaGraphInstantiate(&exec_, g_, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "BC level graph instantiate");
+        return GK_OK;
+    }
+    void abort() {
+        if (capturing_) {
+            cudaGraph_t body = nullptr;
+            cudaStreamEndCapture(cs_, &body);
+            capturing_ = false;
+        }
+        cudaGetLastError();
+    }
+    int launch(cudaStream_t s) {
+        cudaError_t e = cudaGraphLaunch(exec_, s);
+        return e == cudaSuccess ? GK_OK : cuda_fail(e, "BC level graph launch");
+    }
+
+private:
+    cudaGraph_t g_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaStream_t cs_ = nullptr;
+    bool capturing_ = false;
+};
+
 template <int T>
-static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc, cudaStream_t s, Scratch &scr) {
+static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc, const BcOptions &opt,
+                    cudaStream_t s) {
     constexpr int W = 32 * T;
     const int64_t m = g.A.m;
+    const int64_t nnz = g.A.nnz;
     const int sms = ctx().num_sms;
     double *sigma, *R;
     uint32_t *V, *act;
-    unsigned *progress;
+    BcState *st;
+    uint32_t **fptr_dev;
+    float *feat_dev = nullptr;
     Scratch local(s);
     GK_CHECK(local.alloc(&sigma, (size_t)m * W));
     GK_CHECK(local.alloc(&R, (size_t)m * W));
     GK_CHECK(local.alloc(&V, (size_t)m * T));
     GK_CHECK(local.alloc(&act, T));
-    GK_CHECK(local.alloc(&progress, 1));
+    GK_CHECK(local.alloc(&st, 1));
+    if (opt.level_feat && opt.log_cap > 0) GK_CHECK(local.alloc(&feat_dev, (size_t)opt.log_cap * BC_FEAT));
     GK_CUDA(cudaMemsetAsync(V, 0, sizeof(uint32_t) * m * T, s));
+    GK_CUDA(cudaMemsetAsync(sigma, 0, sizeof(double) * m * W, s));  // push levels add into it
+    GK_CUDA(cudaMemsetAsync(st, 0, sizeof(BcState), s));
     uint32_t hact[16];
     for (int t = 0; t < T; ++t) {
         const int lo = 32 * t;
@@ -329,71 +735,211 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
         hact[t] = cnt == 32 ? 0xFFFFFFFFu : ((1u << cnt) - 1u);
     }
     GK_CUDA(cudaMemcpyAsync(act, hact, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, s));
-    std::vector<uint32_t *> levels;
-    auto new_level = [&](uint32_t **out) -> int {
-        uint32_t *p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, sizeof(uint32_t) * m * T, s);
-        if (e != cudaSuccess) return cuda_fail(e, "BC level bitmap");
-        levels.push_back(p);
-        e = cudaMemsetAsync(p, 0, sizeof(uint32_t) * m * T, s);
-        if (e != cudaSuccess) return cuda_fail(e, "BC level bitmap");
-        *out = p;
+
+    // level bitmaps, allocated BC_LEVEL_BATCH at a time; fptr[0] unused
+    std::vector<uint32_t *> levels(1, nullptr);
+    size_t fcap = 0;
+    fptr_dev = nullptr;
+    auto release = [&]() {
+        for (size_t i = 1; i < levels.size(); ++i) cudaFreeAsync(levels[i], s);
+        if (fptr_dev) cudaFreeAsync(fptr_dev, s);
+    };
+    auto grow = [&]() -> int {
+        const size_t want = levels.size() + BC_LEVEL_BATCH;
+        for (int k = 0; k < BC_LEVEL_BATCH; ++k) {
+            uint32_t *p = nullptr;
+            cudaError_t e = cudaMallocAsync(&p, sizeof(uint32_t) * m * T, s);
+            if (e != cudaSuccess) return cuda_fail(e, "BC level bitmap");
+            levels.push_back(p);
+            e = cudaMemsetAsync(p, 0, sizeof(uint32_t) * m * T, s);
+            if (e != cudaSuccess) return cuda_fail(e, "BC level bitmap");
+        }
+        if (want > fcap) {
+            uint32_t **np = nullptr;
+            const size_t ncap = want * 2;
+            cudaError_t e = cudaMallocAsync(&np, sizeof(uint32_t *) * ncap, s);
+            if (e != cudaSuccess) return cuda_fail(e, "BC level table");
+            if (fptr_dev) cudaFreeAsync(fptr_dev, s);
+            fptr_dev = np;
+            fcap = ncap;
+        }
+        cudaError_t e = cudaMemcpyAsync(fptr_dev, levels.data(), sizeof(uint32_t *) * levels.size(),
+                                        cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&st->fptr, &fptr_dev, sizeof(uint32_t **), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "BC level table");
+        const int nlev = static_cast<int>(levels.size()) - 1;
+        // the host's pointer and level count must stay alive until the copies ran
+        e = cudaMemcpyAsync(&st->levels, &nlev, sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_fail(e, "BC level table");
         return GK_OK;
     };
-    auto free_levels = [&]() {
-        for (uint32_t *p : levels) cudaFreeAsync(p, s);
-        levels.clear();
-    };
-    unsigned *h_prog;
-    GK_CUDA(cudaMallocHost(&h_prog, sizeof(unsigned)));
     int status = GK_OK;
     do {
-        uint32_t *F1;
-        if ((status = new_level(&F1)) != GK_OK) break;
-        k_bc_seed<<<sms * 4, 256, 0, s>>>(g.A, src, nsrc, T, W, F1, V, sigma);
-        note_launches(1);
-        // forward sweep: one level per launch pair, until the frontier is empty
-        for (int64_t d = 1; d <= m; ++d) {
-            uint32_t *Fn;
-            if ((status = new_level(&Fn)) != GK_OK) break;
-            cudaMemsetAsync(progress, 0, sizeof(unsigned), s);
-            const uint32_t *Fd = levels[levels.size() - 2];
-            k_bc_forward<T><<<sms * 8, 256, 0, s>>>(g.AT, Fd, Fn, V, sigma, W, act, progress);
-            note_launches(1);
+        if ((status = grow()) != GK_OK) break;
+        k_bc_seed<<<sms * 4, 256, 0, s>>>(g.A, src, nsrc, T, W, levels[1], V, sigma);
+        k_bc_first_stats<T><<<sms * 4, 256, 0, s>>>(g.A, levels[1], st, nsrc);
+        {
+            const int one = 1;
+            GK_CUDA(cudaMemcpyAsync(&st->d, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+            GK_CUDA(cudaStreamSynchronize(s));
+        }
+        note_launches(2);
+
+        // ---- forward levels ----
+        auto fwd_level = [&](cudaStream_t ls, cudaGraphConditionalHandle h, bool in_graph) {
+            k_bc_choose<<<1, 1, 0, ls>>>(st, opt.force, opt.sched, m, nnz, W, feat_dev, opt.log_cap);
+            k_bc_pull<T><<<sms * 8, 256, 0, ls>>>(g.AT, g.A, st, V, sigma, W, act);
             if (g.nheavyAT)
-                k_bc_forward_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, s>>>(g.AT, g.heavyAT, g.nheavyAT, Fd, Fn, V,
-                                                                         sigma, W, act, progress);
-                note_launches(1);
-            cudaMemcpyAsync(h_prog, progress, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
-            cudaError_t e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) {
-                status = cuda_fail(e, "BC forward level");
-                break;
+                k_bc_pull_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.AT, g.A, g.heavyAT, g.nheavyAT, st, V,
+                                                                       sigma, W, act);
+            k_bc_push<T><<<sms * 8, 256, 0, ls>>>(g.A, st, V, sigma, W);
+            if (g.nheavyA)
+                k_bc_push_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.heavyA, g.nheavyA, st, V, sigma,
+                                                                       W);
+            k_bc_push_finish<T><<<sms * 4, 256, 0, ls>>>(g.A, st, V);
+            k_bc_fwd_end<<<1, 1, 0, ls>>>(st, m, h, in_graph ? 1 : 0);
+            return 5 + (g.nheavyAT ? 1 : 0) + (g.nheavyA ? 1 : 0);
+        };
+        BcState hs{};
+        bool graph_ok = !opt.host_loop && !prof_any();
+        LevelGraph fg;
+        cudaGraphConditionalHandle fh{};
+        int per_level = 0;
+        if (graph_ok) {
+            graph_ok = fg.begin(&fh);
+            if (graph_ok) {
+                per_level = fwd_level(fg.stream(), fh, true);
+                if (fg.end() != GK_OK) {
+                    fg.abort();
+                    graph_ok = false;
+                }
+            } else {
+                fg.abort();
             }
-            if (*h_prog == 0) break;  // F_{d+1} empty: levels 1..d are the BFS layers
+        }
+        int lvl_count = 0;
+        std::vector<cudaEvent_t> evs;
+        while (true) {
+            GK_CUDA(cudaMemcpyAsync(&hs, st, sizeof(BcState), cudaMemcpyDeviceToHost, s));
+            GK_CUDA(cudaStreamSynchronize(s));
+            if (hs.done || hs.d >= m) break;
+            if (hs.d + 1 > hs.levels) {
+                if ((status = grow()) != GK_OK) break;
+                continue;
+            }
+            if (graph_ok) {
+                const int d0 = hs.d;
+                if ((status = fg.launch(s)) != GK_OK) break;
+                GK_CUDA(cudaMemcpyAsync(&hs, st, sizeof(BcState), cudaMemcpyDeviceToHost, s));
+                GK_CUDA(cudaStreamSynchronize(s));
+                note_launches(per_level * (hs.d - d0 + (hs.done ? 1 : 0)));
+                if (hs.done) break;
+                continue;
+            }
+            // host-driven level (profiling, autotuning, or no conditional graphs)
+            cudaEvent_t a = nullptr, b = nullptr;
+            if (opt.level_ms) {
+                cudaEventCreate(&a);
+                cudaEventCreate(&b);
+                cudaEventRecord(a, s);
+            }
+            note_launches(fwd_level(s, cudaGraphConditionalHandle{}, false));
+            if (opt.level_ms) {
+                cudaEventRecord(b, s);
+                evs.push_back(a);
+                evs.push_back(b);
+            }
+            ++lvl_count;
         }
         if (status != GK_OK) break;
-        // levels = [F_1 .. F_D, empty]
-        const int D = static_cast<int>(levels.size()) - 1;
-        k_bc_rinit<T><<<sms * 8, 256, 0, s>>>(m, levels[D - 1], sigma, R, W);
+        if (opt.level_ms || opt.level_mode) {
+            GK_CUDA(cudaStreamSynchronize(s));
+            const int n = static_cast<int>(evs.size() / 2);
+            for (int i = 0; i < n && i < opt.log_cap; ++i) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, evs[2 * i], evs[2 * i + 1]);
+                if (opt.level_ms) opt.level_ms[i] = ms;
+            }
+            if (opt.levels_out) *opt.levels_out = n;
+        }
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+        if (opt.level_feat && feat_dev) {
+            const int n = hs.d - 1 + (hs.done ? 1 : 0);
+            const int k = n < opt.log_cap ? n : opt.log_cap;
+            if (k > 0)
+                GK_CUDA(cudaMemcpyAsync(opt.level_feat, feat_dev, sizeof(float) * k * BC_FEAT, cudaMemcpyDeviceToHost,
+                                        s));
+            GK_CUDA(cudaStreamSynchronize(s));
+        }
+
+        // ---- backward levels: D = hs.d ----
+        const int D = hs.d;
+        k_bc_rinit<T><<<sms * 8, 256, 0, s>>>(m, st, sigma, R, W);
         note_launches(1);
-        for (int d = D - 1; d >= 1; --d) {
-            k_bc_backward<T><<<sms * 8, 256, 0, s>>>(g.A, levels[d - 1], levels[d], sigma, R, W, bc);
-            note_launches(1);
+        if (D - 1 < 1) break;
+        {
+            const int bd = D - 1;
+            GK_CUDA(cudaMemcpyAsync(&st->bd, &bd, sizeof(int), cudaMemcpyHostToDevice, s));
+            GK_CUDA(cudaStreamSynchronize(s));
+        }
+        auto bwd_level = [&](cudaStream_t ls, cudaGraphConditionalHandle h, bool in_graph) {
+            k_bc_backward<T><<<sms * 8, 256, 0, ls>>>(g.A, st, sigma, R, W, bc);
             if (g.nheavyA)
-                k_bc_backward_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, s>>>(g.A, g.heavyA, g.nheavyA, levels[d - 1],
-                                                                          levels[d], sigma, R, W, bc);
-                note_launches(1);
+                k_bc_backward_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.heavyA, g.nheavyA, st, sigma, R,
+                                                                           W, bc);
+            k_bc_bwd_end<<<1, 1, 0, ls>>>(st, h, in_graph ? 1 : 0);
+            return 2 + (g.nheavyA ? 1 : 0);
+        };
+        bool bgraph = !opt.host_loop && !prof_any();
+        LevelGraph bg;
+        cudaGraphConditionalHandle bh{};
+        int per_b = 0;
+        if (bgraph) {
+            bgraph = bg.begin(&bh);
+            if (bgraph) {
+                per_b = bwd_level(bg.stream(), bh, true);
+                if (bg.end() != GK_OK) {
+                    bg.abort();
+                    bgraph = false;
+                }
+            } else {
+                bg.abort();
+            }
+        }
+        if (bgraph) {
+            if ((status = bg.launch(s)) != GK_OK) break;
+            note_launches(per_b * (D - 1));
+        } else {
+            for (int d = D - 1; d >= 1; --d) note_launches(bwd_level(s, cudaGraphConditionalHandle{}, false));
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) status = cuda_fail(e, "BC backward");
     } while (false);
-    free_levels();
-    cudaFreeHost(h_prog);
+    cudaError_t e = cudaStreamSynchronize(s);
+    release();
+    if (status == GK_OK && e != cudaSuccess) status = cuda_fail(e, "BC chunk");
     return status;
 }
 
-int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, cudaStream_t s, Scratch &scr) {
+static int ensure_bc_model(int sched) {
+    if (sched != GK_SCHED_LEARNED) return GK_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_bc_model_mutex);
+    if (g_bc_model.empty())
+        return fail(GK_ERR_ARG, "learned BC scheduling requested but no model is loaded (gk_bc_set_model)");
+    if (g_bc_uploaded[dev & 63] != g_bc_model_version) {
+        GK_CUDA(cudaMemcpyToSymbol(d_mlp_bc, g_bc_model.data(), sizeof(float) * MLP_SIZE));
+        g_bc_uploaded[dev & 63] = g_bc_model_version;
+    }
+    return GK_OK;
+}
+
+int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const BcOptions &opt, cudaStream_t s,
+              Scratch &scr) {
+    if (opt.sched != GK_SCHED_PLAIN && opt.sched != GK_SCHED_LEARNED) return fail(GK_ERR_ARG, "unknown scheduler mode");
+    GK_CHECK(ensure_bc_model(opt.sched));
     const int sms = ctx().num_sms;
     BcBuffers g;
     g.A = A;
@@ -430,11 +976,11 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, cudaStr
         const int n = left < 32 * T ? left : 32 * T;
         int st;
         switch (T) {
-            case 16: st = bc_chunk<16>(g, src + done, n, bc, s, scr); break;
-            case 8: st = bc_chunk<8>(g, src + done, n, bc, s, scr); break;
-            case 4: st = bc_chunk<4>(g, src + done, n, bc, s, scr); break;
-            case 2: st = bc_chunk<2>(g, src + done, n, bc, s, scr); break;
-            default: st = bc_chunk<1>(g, src + done, n, bc, s, scr); break;
+            case 16: st = bc_chunk<16>(g, src + done, n, bc, opt, s); break;
+            case 8: st = bc_chunk<8>(g, src + done, n, bc, opt, s); break;
+            case 4: st = bc_chunk<4>(g, src + done, n, bc, opt, s); break;
+            case 2: st = bc_chunk<2>(g, src + done, n, bc, opt, s); break;
+            default: st = bc_chunk<1>(g, src + done, n, bc, opt, s); break;
         }
         GK_CHECK(st);
         done += n;
@@ -442,13 +988,9 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, cudaStr
     return GK_OK;
 }
 
-}  // namespace gk
-
-using namespace gk;
-
-extern "C" int gk_bc_batch(const gk_csr *A, const int32_t *sources, int nsources, double *bc, int sched,
-                           void *stream) {
-    (void)sched;  // the BC sweep has one kernel shape per level; the scheduler is not consulted
+// Validates A and the sources, stages them, runs the batch.
+static int bc_entry(const gk_csr *A, const int32_t *sources, int nsources, double *bc, const BcOptions &opt,
+                    void *stream) {
     GK_CHECK(validate_csr_shape(A, "A"));
     if (A->m != A->n) return fail(GK_ERR_ARG, "non-square matrix; BC is only for square matrices");
     if (nsources < 0 || (nsources > 0 && !sources) || (A->m > 0 && !bc)) return fail(GK_ERR_ARG, "bad arguments");
@@ -476,10 +1018,55 @@ extern "C" int gk_bc_batch(const gk_csr *A, const int32_t *sources, int nsources
     const bool host_out = A->m > 0 && !is_device_pointer(bc);
     double *dbc = bc;
     if (host_out) GK_CHECK(scr.alloc(&dbc, A->m));
-    if (A->m > 0) GK_CHECK(bc_device(d, dsrc, nsources, dbc, s, scr));
+    if (A->m > 0) GK_CHECK(bc_device(d, dsrc, nsources, dbc, opt, s, scr));
     if (host_out) {
         GK_CUDA(cudaMemcpyAsync(bc, dbc, sizeof(double) * A->m, cudaMemcpyDeviceToHost, s));
-        GK_CUDA(cudaStreamSynchronize(s));
     }
+    GK_CUDA(cudaStreamSynchronize(s));
     return GK_OK;
+}
+
+}  // namespace gk
+
+using namespace gk;
+
+extern "C" int gk_bc_batch(const gk_csr *A, const int32_t *sources, int nsources, double *bc, int sched,
+                           void *stream) {
+    BcOptions opt;
+    opt.sched = sched;
+    return bc_entry(A, sources, nsources, bc, opt, stream);
+}
+
+extern "C" int gk_bc_tune(const gk_csr *A, const int32_t *sources, int nsources, int shape, double *bc,
+                          float *level_ms, float *level_feat, int max_levels, int *nlevels, void *stream) {
+    if (shape < -1 || shape > 1) return fail(GK_ERR_ARG, "gk_bc_tune: shape must be -1, 0 (pull) or 1 (push)");
+    if (max_levels < 0 || (max_levels > 0 && (!level_ms || !level_feat)) || !nlevels)
+        return fail(GK_ERR_ARG, "gk_bc_tune: bad level arrays");
+    if (nsources > 512) return fail(GK_ERR_ARG, "gk_bc_tune: at most 512 sources (one chunk)");
+    BcOptions opt;
+    opt.sched = GK_SCHED_PLAIN;
+    opt.force = shape;
+    opt.host_loop = true;
+    opt.level_ms = level_ms;
+    opt.level_feat = level_feat;
+    opt.log_cap = max_levels;
+    opt.levels_out = nlevels;
+    *nlevels = 0;
+    return bc_entry(A, sources, nsources, bc, opt, stream);
+}
+
+extern "C" int gk_bc_set_model(const float *weights, size_t n_floats) {
+    if (!weights || n_floats != static_cast<size_t>(MLP_SIZE))
+        return fail(GK_ERR_ARG, "gk_bc_set_model: weight count does not match gk_sched_model_size()");
+    for (size_t i = 0; i < n_floats; ++i)
+        if (!std::isfinite(weights[i])) return fail(GK_ERR_ARG, "gk_bc_set_model: non-finite weight");
+    std::lock_guard<std::mutex> lock(g_bc_model_mutex);
+    g_bc_model.assign(weights, weights + n_floats);
+    ++g_bc_model_version;
+    return GK_OK;
+}
+
+extern "C" int gk_bc_has_model(void) {
+    std::lock_guard<std::mutex> lock(g_bc_model_mutex);
+    return g_bc_model.empty() ? 0 : 1;
 }

@@ -154,6 +154,8 @@ static std::vector<Pending> g_pending;
 
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 bool prof_enabled() { return g_prof_on.load(std::memory_order_relaxed) == 1; }
+bool prof_any() { return g_prof_on.load(std::memory_order_relaxed) != 0; }
+int64_t launches_noted() { return g_launches.load(std::memory_order_relaxed); }
 static bool prof_events_only() { return g_prof_on.load(std::memory_order_relaxed) == 2; }
 
 ProfWindow::ProfWindow(cudaStream_t s, int slots) : s_(s), on_(prof_enabled()), slots_(slots < 64 ? slots : 64) {

@@ -99,6 +99,8 @@ SideStreams &side_streams();
 // ----- launch counter and per-variant profiling (gk_launch_count, gk_prof_*) ----
 void note_launches(int n);
 bool prof_enabled();
+bool prof_any();          // any profiling mode (its events cannot be captured into graphs)
+int64_t launches_noted();  // kernel launches counted so far
 
 struct ProfTotals {
     unsigned long long rows, sum_a, sum_m, sum_work;

@@ -15,6 +15,13 @@ namespace gk {
 
 constexpr int EMPTY_KEY = -1;
 
+// When a row's mask is processed in chunks (column ranges), a B row longer
+// than this is cut to the chunk's column range by two group searches; a
+// shorter one is streamed whole, since its columns outside the range are not
+// in the chunk's structure and cost less to test than the searches' round
+// trips to memory.
+constexpr int64_t CUT_MIN = 256;
+
 // Lanes of the calling thread's aligned group of G threads inside its warp.
 template <int G>
 __device__ __forceinline__ unsigned group_mask() {
@@ -32,46 +39,71 @@ __device__ __forceinline__ unsigned low_bits() {
     else return (1u << G) - 1u;
 }
 
-// Multiplicative (Fibonacci) hashing of a column index into 2^LOG2 slots.
-template <int CAP>
-__device__ __forceinline__ int hash_slot(int x) {
-    constexpr int LOG2 = __builtin_ctz(CAP);
-    return static_cast<int>((static_cast<uint32_t>(x) * 0x9E3779B1u) >> (32 - LOG2));
-}
-
 // Bit of x in a 2^FLOG-bit filter (a second multiplicative hash, independent
-// of the table slot's).
+// of the table's bucket hash).
 template <int FLOG>
 __device__ __forceinline__ uint32_t filter_bit(int x) {
     return (static_cast<uint32_t>(x) * 0x85EBCA77u) >> (32 - FLOG);
 }
 
-// Inserts x into an open-addressing (linear probing) table; concurrent
-// inserts of distinct keys are safe.  The caller guarantees fewer than CAP
-// keys, so a free slot always exists; the probe count is bounded anyway.
+// The mask tables are bucketed open addressing: CAP slots as CAP/4 buckets
+// of four adjacent slots, read with one 16-byte shared-memory load.  A key
+// lives in its home bucket or, when that bucket is full, in the following
+// ones (linear probing over buckets).  The slots of a bucket fill in order,
+// so a bucket with an empty last slot ends every probe sequence.
+template <int CAP>
+__device__ __forceinline__ int home_bucket(int x) {
+    constexpr int LOG2 = __builtin_ctz(CAP / 4);
+    static_assert(CAP >= 8 && (CAP & (CAP - 1)) == 0, "table size must be a power of two >= 8");
+    return static_cast<int>((static_cast<uint32_t>(x) * 0x9E3779B1u) >> (32 - LOG2));
+}
+
+// Inserts x; concurrent inserts of distinct keys are safe (a slot is claimed
+// by compare-and-swap only after the slots before it were seen taken).  The
+// caller guarantees fewer than CAP keys; the probe count is bounded anyway.
 template <int CAP>
 __device__ __forceinline__ void hash_insert(int *keys, int x) {
-    int s = hash_slot<CAP>(x);
+    int b = home_bucket<CAP>(x);
 #pragma unroll 1
-    for (int probe = 0; probe < CAP; ++probe) {
-        const int prev = atomicCAS(keys + s, EMPTY_KEY, x);
-        if (prev == EMPTY_KEY || prev == x) return;
-        s = (s + 1) & (CAP - 1);
+    for (int probe = 0; probe < CAP / 4; ++probe) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int prev = atomicCAS(keys + 4 * b + i, EMPTY_KEY, x);
+            if (prev == EMPTY_KEY || prev == x) return;
+        }
+        b = (b + 1) & (CAP / 4 - 1);
     }
 }
 
 // Slot of x, or -1 when x is not a key.
 template <int CAP>
 __device__ __forceinline__ int hash_find(const int *keys, int x) {
-    int s = hash_slot<CAP>(x);
+    int b = home_bucket<CAP>(x);
 #pragma unroll 1
-    for (int probe = 0; probe < CAP; ++probe) {
-        const int k = keys[s];
-        if (k == x) return s;
-        if (k == EMPTY_KEY) return -1;
-        s = (s + 1) & (CAP - 1);
+    for (int probe = 0; probe < CAP / 4; ++probe) {
+        const int4 k = *reinterpret_cast<const int4 *>(keys + 4 * b);
+        if (k.x == x) return 4 * b;
+        if (k.y == x) return 4 * b + 1;
+        if (k.z == x) return 4 * b + 2;
+        if (k.w == x) return 4 * b + 3;
+        if (k.w == EMPTY_KEY) return -1;
+        b = (b + 1) & (CAP / 4 - 1);
     }
     return -1;
+}
+
+// Whether x is a key (no slot needed: the sum epilogues).
+template <int CAP>
+__device__ __forceinline__ bool hash_has(const int *keys, int x) {
+    int b = home_bucket<CAP>(x);
+#pragma unroll 1
+    for (int probe = 0; probe < CAP / 4; ++probe) {
+        const int4 k = *reinterpret_cast<const int4 *>(keys + 4 * b);
+        if ((k.x == x) | (k.y == x) | (k.z == x) | (k.w == x)) return true;
+        if (k.w == EMPTY_KEY) return false;
+        b = (b + 1) & (CAP / 4 - 1);
+    }
+    return false;
 }
 
 // Index of x in sorted keys[0, n), or -1.

@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
                     if (tnn < t1) k2 = __ldg(p.A.col + tnn);
                     if (cur.b0 < cur.b1) {
                         bool skip = false;
-                        if (cut) {
+                        if (cut && cur.b1 - cur.b0 > CUT_MIN) {
                             skip = __ldg(p.B.col + cur.b1 - 1) < lo_col || __ldg(p.B.col + cur.b0) > hi_col;
                             if (!skip) {
                                 const int64_t lo = group_lower_bound<SUB>(p.B.col, cur.b0, cur.b1, lo_col, sl, smask);

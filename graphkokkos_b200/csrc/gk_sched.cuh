@@ -46,11 +46,14 @@ struct Variant {
     int accum;      // gk_accum family this variant belongs to
 };
 
-constexpr int NV = 13;
+constexpr int NV = 15;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
-// Hash tables without a filter run at load factor <= 1/4 (chunk <= cap/4);
-// behind a filter of about 64 bits per mask entry only filter candidates
-// reach the table, and the large tables of variants 6-8 run at load <= 1/2.
+// Tables are bucketed (four slots per 16-byte load).  The small ones run at
+// load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
+// 12-14 at load <= 1/2.  Variants with a filter (about 64 bits per mask
+// entry) send only filter candidates to the table; variants 12-14 have none
+// and look every streamed element up in the table directly, which wins on
+// rows where a large share of the elements are mask columns.
 // columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum
 #define GK_VARIANT_TABLE { \
     {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3},   \
@@ -59,13 +62,15 @@ constexpr int NV = 13;
     {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3},   \
     {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
     {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
-    {K_HASH_BLOCK, 128, 32,  2048,  4096,  1024,  1024,  18, 16, 2, 3},   \
-    {K_HASH_BLOCK, 256, 32,  8192, 16384,  4096,  4096,  19, 17, 1, 3},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  4096,  20, 18, 1, 3},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 16, 2, 3},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19, 17, 1, 3},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3},   \
     {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2},   \
     {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2},   \
     {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1},   \
     {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18,  0, 2, 3},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3},   \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -96,6 +101,8 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 10: return qm >= 7;
         case 11: return qm >= 9;
         case 12: return qm >= 5;
+        case 13: return true;
+        case 14: return qm >= 8;
         default: return false;
     }
 }
@@ -112,5 +119,11 @@ constexpr int MLP_H = 32;
 // layout (float32): W1[MLP_H][NFEAT], b1[MLP_H], W2[MLP_H][MLP_H], b2[MLP_H],
 //                   W3[NV][MLP_H], b3[NV], mu[NFEAT], sigma[NFEAT]
 constexpr int MLP_SIZE = MLP_H * NFEAT + MLP_H + MLP_H * MLP_H + MLP_H + NV * MLP_H + NV + 2 * NFEAT;
+
+#ifdef __CUDACC__
+// Forward pass of the network (mlp.cu): out[NV] from the raw features f;
+// x, h1, h2 are caller scratch of NFEAT, MLP_H, MLP_H floats.
+__device__ void mlp_forward(const float *w, const float *f, float *x, float *h1, float *h2, float *out);
+#endif
 
 }  // namespace gk

@@ -37,9 +37,18 @@ struct SpgemmRequest {
 
 int run_spgemm(const SpgemmRequest &req, Scratch &scr);
 
+// Everything run_spgemm configures on its first use (kernel attributes and
+// grid sizes of every variant for this epilogue, the learned model's upload),
+// done ahead so that later calls can be captured into a CUDA graph.
+int spgemm_prepare(int epi, bool values, int sched, int force_accum);
+// Device scratch one run_spgemm call on an m-row A takes (arena sizing).
+size_t spgemm_scratch_bytes(int64_t m);
+
 // Scheduler (sched.cu): fills var_of_bin[NBINS] on the device from the bin
 // statistics, by the plain heuristic, the learned MLP, or a forced family.
 int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_accum, int epi, bool values,
                  cudaStream_t s);
+// Validates the mode and uploads the learned model if it will be used.
+int sched_prepare(int sched, int force_accum);
 
 }  // namespace gk

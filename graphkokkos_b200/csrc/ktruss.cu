@@ -8,10 +8,14 @@
 //   2. flag     keep[j] = S[j] >= k-2
 //   3. scan     exclusive prefix of keep over all entries (one device scan)
 //   4. compact  new_rp[i] = pos[rp[i]], new_col[pos[j]] = col[j] for kept j
+//   5. copy the pruned matrix back over the current one
 // and the loop stops when the kept count equals nnz.  Compaction preserves the
 // order within rows, so rows stay sorted and the edge set is bit-exact with the
 // reference (whose View-size defect at :99/:118 is not reproduced).
-// The host reads the kept count once per pass to decide whether to stop.
+// Every pass reads its sizes on the device, so the loop is one CUDA graph: a
+// conditional while node around one captured pass, the condition set by the
+// pass's last kernel; the host waits once, at the end.  With profiling on
+// (its events cannot be captured) the host runs the passes itself.
 #include <cub/cub.cuh>
 
 #include "gk_common.cuh"
@@ -19,91 +23,192 @@
 
 namespace gk {
 
-__global__ void k_keep_flags(const int32_t *sup, int64_t nnz, int thresh, int32_t *keep) {
+// Loop state in device memory, so that a pass needs no host value.
+struct KtState {
+    long long iters;   // passes run
+    long long kept;    // nnz after the last pass
+};
+
+// keep[j] = S[j] >= k-2 for j < nnz (nnz = rp[m]); 0 up to the capacity, so
+// that a scan over capacity+1 entries yields the kept count at pos[cap].
+__global__ void k_keep_flags(const int32_t *sup, const int64_t *rp, int64_t m, int64_t cap, int thresh,
+                             int32_t *keep) {
+    const int64_t nnz = rp[m];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += stride)
-        keep[j] = sup[j] >= thresh;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= cap; j += stride)
+        keep[j] = j < nnz ? (sup[j] >= thresh) : 0;
 }
 
-__global__ void k_compact(int64_t m, int64_t nnz, const int64_t *rp, const int32_t *col, const int32_t *keep,
-                          const int64_t *pos, int64_t *nrp, int32_t *ncol) {
+__global__ void k_compact(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *keep, const int64_t *pos,
+                          int64_t *nrp, int32_t *ncol) {
+    const int64_t nnz = rp[m];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += stride)
         if (keep[j]) ncol[pos[j]] = col[j];
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= m; i += stride) nrp[i] = pos[rp[i]];
 }
 
+// End of a pass: count it and decide whether another pass follows (the edge
+// count changed and fewer than max_iters passes ran).  Inside the graph the
+// decision drives the conditional while node.
+__global__ void k_pass_end(const int64_t *rp, const int64_t *nrp, int64_t m, long long max_iters, KtState *st,
+                           cudaGraphConditionalHandle h, int in_graph) {
+    const long long old = rp[m], kept = nrp[m];
+    const long long it = st->iters + 1;
+    st->iters = it;
+    st->kept = kept;
+    if (in_graph) cudaGraphSetConditional(h, (kept != old && it < max_iters) ? 1u : 0u);
+}
+
+// The pruned matrix becomes the current one.
+__global__ void k_copy_back(int64_t m, const int64_t *nrp, const int32_t *ncol, int64_t *rp, int32_t *col) {
+    const int64_t nnz = nrp[m];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= m; i += stride) rp[i] = nrp[i];
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += stride) col[j] = ncol[j];
+}
+
+struct KtBuffers {
+    int64_t m, cap;            // rows, nnz of the input (capacity of every edge array)
+    int64_t *rp, *nrp;         // current / pruned row pointers
+    int32_t *col, *ncol;       // current / pruned columns
+    int32_t *sup, *keep;       // support per entry, keep flags (cap + 1)
+    int64_t *pos;              // exclusive scan of keep (cap + 1)
+    void *scan_tmp;
+    size_t scan_bytes;
+    void *arena;               // scratch of the support SpGEMM
+    size_t arena_bytes;
+    KtState *st;
+    int k, sched;
+};
+
+// One pass: support S<C> = C·C, flags, scan, compaction, pass end, copy back.
+// Every size is read on the device, so the same launches serve every pass.
+static int ktruss_pass(const KtBuffers &b, cudaStream_t s, cudaGraphConditionalHandle h, bool in_graph) {
+    const int sms = ctx().num_sms;
+    Scratch pass(s, b.arena, b.arena_bytes);
+    SpgemmRequest rq;
+    DevCsr c{b.m, b.m, b.cap, b.rp, b.col, nullptr};
+    rq.A = rq.B = rq.M = c;
+    rq.epi = EPI_WRITE;
+    rq.sched = b.sched;
+    rq.c_val = b.sup;
+    rq.stream = s;
+    GK_CHECK(run_spgemm(rq, pass));
+    k_keep_flags<<<sms * 8, 256, 0, s>>>(b.sup, b.rp, b.m, b.cap, b.k - 2, b.keep);
+    size_t scan_bytes = b.scan_bytes;
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, scan_bytes, b.keep, b.pos, b.cap + 1, s));
+    k_compact<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.col, b.keep, b.pos, b.nrp, b.ncol);
+    k_pass_end<<<1, 1, 0, s>>>(b.rp, b.nrp, b.m, static_cast<long long>(b.m), b.st, h, in_graph ? 1 : 0);
+    k_copy_back<<<sms * 8, 256, 0, s>>>(b.m, b.nrp, b.ncol, b.rp, b.col);
+    note_launches(5);
+    GK_CUDA(cudaGetLastError());
+    return GK_OK;
+}
+
+// The whole loop as one CUDA graph: a conditional while node whose body is
+// one pass, captured once.  Returns GK_ERR_UNSUPPORTED where the graph cannot
+// be built (the caller then runs the passes from the host).
+static int ktruss_graph(const KtBuffers &b, cudaStream_t s, int *passes_per_launch) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cs = nullptr;
+    int status = GK_OK;
+    do {
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) { status = GK_ERR_UNSUPPORTED; break; }
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            status = GK_ERR_UNSUPPORTED;
+            break;
+        }
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess) { status = GK_ERR_UNSUPPORTED; break; }
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { status = GK_ERR_UNSUPPORTED; break; }
+        if (cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+            cudaSuccess) {
+            status = GK_ERR_UNSUPPORTED;
+            break;
+        }
+        const int64_t before = launches_noted();
+        const int ps = ktruss_pass(b, cs, h, true);
+        *passes_per_launch = static_cast<int>(launches_noted() - before);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+        if (ps != GK_OK) { status = ps; break; }
+        if (ce != cudaSuccess) { status = cuda_fail(ce, "k-truss pass capture"); break; }
+        if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+            cudaGetLastError();
+            status = GK_ERR_UNSUPPORTED;
+            break;
+        }
+        const cudaError_t le = cudaGraphLaunch(exec, s);
+        if (le != cudaSuccess) status = cuda_fail(le, "k-truss graph launch");
+    } while (false);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g) cudaGraphDestroy(g);
+    if (cs) cudaStreamDestroy(cs);
+    return status;
+}
+
 int ktruss_device(int64_t m, int64_t nnz0, int64_t *rp_a, int32_t *col_a, int k, int sched, int *iters_out,
                   int64_t *nnz_out, int64_t **rp_res, int32_t **col_res, cudaStream_t s, Scratch &scr) {
-    int64_t *rp_b;
-    int32_t *col_b, *sup, *keep;
-    int64_t *pos;
-    GK_CHECK(scr.alloc(&rp_b, m + 1));
-    GK_CHECK(scr.alloc(&col_b, nnz0 > 0 ? nnz0 : 1));
-    GK_CHECK(scr.alloc(&sup, nnz0 > 0 ? nnz0 : 1));
-    GK_CHECK(scr.alloc(&keep, nnz0 + 1));
-    GK_CHECK(scr.alloc(&pos, nnz0 + 1));
-    size_t tb = 0;
-    GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, keep, pos, nnz0 + 1, s));
-    void *tmp;
-    GK_CHECK(scr.alloc(reinterpret_cast<char **>(&tmp), tb));
-    const int sms = ctx().num_sms;
-    int64_t *rp_cur = rp_a, *rp_nxt = rp_b;
-    int32_t *col_cur = col_a, *col_nxt = col_b;
-    int64_t nnz = nnz0;
-    int iters = 0;
-    int64_t *h_nnz;
-    GK_CUDA(cudaMallocHost(&h_nnz, sizeof(int64_t)));
-    int status = GK_OK;
-    for (int64_t t = 0; t < m; ++t) {
-        if (nnz == 0) {
-            ++iters;
-            break;
-        }
-        // the scheduler's plan arrays live for one pass only
-        Scratch pass(s);
-        SpgemmRequest rq;
-        DevCsr c{m, m, nnz, rp_cur, col_cur, nullptr};
-        rq.A = rq.B = rq.M = c;
-        rq.epi = EPI_WRITE;
-        rq.sched = sched;
-        rq.c_val = sup;
-        rq.stream = s;
-        status = run_spgemm(rq, pass);
-        if (status != GK_OK) break;
-        k_keep_flags<<<sms * 8, 256, 0, s>>>(sup, nnz, k - 2, keep);
-        note_launches(1);
-        if (cudaMemsetAsync(keep + nnz, 0, sizeof(int32_t), s) != cudaSuccess) {
-            status = cuda_fail(cudaGetLastError(), "memset");
-            break;
-        }
-        cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tb, keep, pos, nnz + 1, s);
-        if (e != cudaSuccess) {
-            status = cuda_fail(e, "ktruss scan");
-            break;
-        }
-        k_compact<<<sms * 8, 256, 0, s>>>(m, nnz, rp_cur, col_cur, keep, pos, rp_nxt, col_nxt);
-        note_launches(1);
-        e = cudaMemcpyAsync(h_nnz, pos + nnz, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-            status = cuda_fail(e, "ktruss pass");
-            break;
-        }
-        ++iters;
-        const int64_t kept = *h_nnz;
-        std::swap(rp_cur, rp_nxt);
-        std::swap(col_cur, col_nxt);
-        const bool same = kept == nnz;
-        nnz = kept;
-        if (same) break;
+    *rp_res = rp_a;
+    *col_res = col_a;
+    if (nnz0 == 0 || m == 0) {  // the reference counts one pass over the empty matrix
+        *iters_out = m > 0 ? 1 : 0;
+        *nnz_out = 0;
+        return GK_OK;
     }
-    cudaFreeHost(h_nnz);
-    if (status != GK_OK) return status;
-    *iters_out = iters;
-    *nnz_out = nnz;
-    *rp_res = rp_cur;
-    *col_res = col_cur;
+    KtBuffers b;
+    b.m = m;
+    b.cap = nnz0;
+    b.rp = rp_a;
+    b.col = col_a;
+    b.k = k;
+    b.sched = sched;
+    GK_CHECK(scr.alloc(&b.nrp, m + 1));
+    GK_CHECK(scr.alloc(&b.ncol, nnz0));
+    GK_CHECK(scr.alloc(&b.sup, nnz0));
+    GK_CHECK(scr.alloc(&b.keep, nnz0 + 1));
+    GK_CHECK(scr.alloc(&b.pos, nnz0 + 1));
+    GK_CHECK(scr.alloc(&b.st, 1));
+    b.scan_bytes = 0;
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b.scan_bytes, b.keep, b.pos, nnz0 + 1, s));
+    GK_CHECK(scr.alloc(reinterpret_cast<char **>(&b.scan_tmp), b.scan_bytes));
+    b.arena_bytes = spgemm_scratch_bytes(m);
+    GK_CHECK(scr.alloc(reinterpret_cast<char **>(&b.arena), b.arena_bytes));
+    GK_CUDA(cudaMemsetAsync(b.st, 0, sizeof(KtState), s));
+    GK_CHECK(spgemm_prepare(EPI_WRITE, false, sched, GK_ACCUM_AUTO));
+
+    int status = GK_ERR_UNSUPPORTED;
+    int per_pass = 0;
+    if (!prof_any()) status = ktruss_graph(b, s, &per_pass);
+    KtState h{};
+    if (status == GK_OK) {
+        GK_CUDA(cudaMemcpyAsync(&h, b.st, sizeof(KtState), cudaMemcpyDeviceToHost, s));
+        GK_CUDA(cudaStreamSynchronize(s));
+        note_launches(static_cast<int>(per_pass * (h.iters - 1)));  // replays beyond the captured pass
+    } else if (status == GK_ERR_UNSUPPORTED) {
+        // passes driven from the host (profiling on, or no conditional graphs)
+        long long prev = nnz0;
+        for (int64_t t = 0; t < m; ++t) {
+            GK_CHECK(ktruss_pass(b, s, cudaGraphConditionalHandle{}, false));
+            GK_CUDA(cudaMemcpyAsync(&h, b.st, sizeof(KtState), cudaMemcpyDeviceToHost, s));
+            GK_CUDA(cudaStreamSynchronize(s));
+            if (h.kept == prev) break;
+            prev = h.kept;
+        }
+    } else {
+        return status;
+    }
+    *iters_out = static_cast<int>(h.iters);
+    *nnz_out = h.kept;
     return GK_OK;
 }
 

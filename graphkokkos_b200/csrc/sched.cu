@@ -135,11 +135,16 @@ static int ensure_model_on_device() {
     return GK_OK;
 }
 
-int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_accum, int epi, bool values,
-                 cudaStream_t s) {
+int sched_prepare(int sched, int force_accum) {
     if (sched != GK_SCHED_PLAIN && sched != GK_SCHED_LEARNED) return fail(GK_ERR_ARG, "unknown scheduler mode");
     if (force_accum < GK_ACCUM_AUTO || force_accum > GK_ACCUM_HASH) return fail(GK_ERR_ARG, "unknown accumulator");
     if (sched == GK_SCHED_LEARNED && force_accum == GK_ACCUM_AUTO) GK_CHECK(ensure_model_on_device());
+    return GK_OK;
+}
+
+int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_accum, int epi, bool values,
+                 cudaStream_t s) {
+    GK_CHECK(sched_prepare(sched, force_accum));
     k_choose<<<1, NBINS, 0, s>>>(bins, var_of_bin, sched, force_accum, epi, values);
     GK_CUDA(cudaGetLastError());
     return GK_OK;

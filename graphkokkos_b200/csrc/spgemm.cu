@@ -241,8 +241,10 @@ __device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, i
         s = (y >= 0 && y < (1 << CAP) && ((reinterpret_cast<const unsigned *>(keys)[y >> 5] >> (y & 31)) & 1u)) ? y : -1;
     } else if constexpr (PK == PK_MCA) {
         s = sorted_find(keys, clen, x);
-    } else {
+    } else if constexpr (ACC) {
         s = hash_find<CAP>(keys, x);
+    } else {
+        s = hash_has<CAP>(keys, x) ? 0 : -1;  // no slot needed without accumulators
     }
     if (s >= 0) {
         if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), w);
@@ -259,10 +261,11 @@ __device__ __forceinline__ uint32_t cand_bit(int x, const unsigned *filt) {
 
 template <int CAP, bool ACC>
 __device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, int *acc, unsigned &cnt) {
-    const int s = hash_find<CAP>(keys, x);
-    if (s >= 0) {
-        if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + s), w);
-        else cnt += w;
+    if constexpr (ACC) {
+        const int s = hash_find<CAP>(keys, x);
+        if (s >= 0) atomicAdd(reinterpret_cast<unsigned *>(acc + s), w);
+    } else {
+        if (hash_has<CAP>(keys, x)) cnt += w;
     }
 }
 
@@ -392,7 +395,7 @@ __device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, in
         if (tn + step < a1) k2 = __ldg(p.A.col + tn + step);
         if (cur.b0 < cur.b1) {
             bool skip = false;
-            if (chunked) {
+            if (chunked && cur.b1 - cur.b0 > CUT_MIN) {
                 skip = __ldg(p.B.col + cur.b1 - 1) < lo_col || __ldg(p.B.col + cur.b0) > hi_col;
                 if (!skip) {
                     const int64_t lo = group_lower_bound<SUB>(p.B.col, cur.b0, cur.b1, lo_col, sl, smask);
@@ -517,8 +520,10 @@ constexpr size_t smem_bytes(bool write) {
     }
 }
 
+// launch == false: only size the grid (attributes and occupancy), so that a
+// later launch inside a stream capture makes no configuration calls.
 template <int V, int EPI, bool VAL>
-static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t s) {
+static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t s, bool launch = true) {
     constexpr Variant X = VARIANTS[V];
     constexpr bool W = (EPI == EPI_WRITE);
     constexpr size_t SMEM = smem_bytes<V>(W);
@@ -550,35 +555,57 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         if (e != cudaSuccess) return e;
         per_sm = n < 1 ? 1 : n;
     }
+    if (!launch) return cudaSuccess;
     fn<<<num_sms * per_sm, nt, SMEM, s>>>(args);
     return cudaGetLastError();
 }
 
 template <int V>
-static cudaError_t launch_variant_v(const KArgs &a, int epi, bool val, int sms, cudaStream_t s) {
-    if (epi == EPI_WRITE) return val ? launch_variant_t<V, EPI_WRITE, true>(a, sms, s)
-                                     : launch_variant_t<V, EPI_WRITE, false>(a, sms, s);
-    if (epi == EPI_SUM) return launch_variant_t<V, EPI_SUM, false>(a, sms, s);
-    return launch_variant_t<V, EPI_KEYED, false>(a, sms, s);
+static cudaError_t launch_variant_v(const KArgs &a, int epi, bool val, int sms, cudaStream_t s, bool launch) {
+    if (epi == EPI_WRITE) return val ? launch_variant_t<V, EPI_WRITE, true>(a, sms, s, launch)
+                                     : launch_variant_t<V, EPI_WRITE, false>(a, sms, s, launch);
+    if (epi == EPI_SUM) return launch_variant_t<V, EPI_SUM, false>(a, sms, s, launch);
+    return launch_variant_t<V, EPI_KEYED, false>(a, sms, s, launch);
 }
 
-static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int sms, cudaStream_t s) {
+static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int sms, cudaStream_t s,
+                                  bool launch = true) {
     switch (v) {
-        case 0: return launch_variant_v<0>(a, epi, val, sms, s);
-        case 1: return launch_variant_v<1>(a, epi, val, sms, s);
-        case 2: return launch_variant_v<2>(a, epi, val, sms, s);
-        case 3: return launch_variant_v<3>(a, epi, val, sms, s);
-        case 4: return launch_variant_v<4>(a, epi, val, sms, s);
-        case 5: return launch_variant_v<5>(a, epi, val, sms, s);
-        case 6: return launch_variant_v<6>(a, epi, val, sms, s);
-        case 7: return launch_variant_v<7>(a, epi, val, sms, s);
-        case 8: return launch_variant_v<8>(a, epi, val, sms, s);
-        case 9: return launch_variant_v<9>(a, epi, val, sms, s);
-        case 10: return launch_variant_v<10>(a, epi, val, sms, s);
-        case 11: return launch_variant_v<11>(a, epi, val, sms, s);
-        case 12: return launch_variant_v<12>(a, epi, val, sms, s);
+        case 0: return launch_variant_v<0>(a, epi, val, sms, s, launch);
+        case 1: return launch_variant_v<1>(a, epi, val, sms, s, launch);
+        case 2: return launch_variant_v<2>(a, epi, val, sms, s, launch);
+        case 3: return launch_variant_v<3>(a, epi, val, sms, s, launch);
+        case 4: return launch_variant_v<4>(a, epi, val, sms, s, launch);
+        case 5: return launch_variant_v<5>(a, epi, val, sms, s, launch);
+        case 6: return launch_variant_v<6>(a, epi, val, sms, s, launch);
+        case 7: return launch_variant_v<7>(a, epi, val, sms, s, launch);
+        case 8: return launch_variant_v<8>(a, epi, val, sms, s, launch);
+        case 9: return launch_variant_v<9>(a, epi, val, sms, s, launch);
+        case 10: return launch_variant_v<10>(a, epi, val, sms, s, launch);
+        case 11: return launch_variant_v<11>(a, epi, val, sms, s, launch);
+        case 12: return launch_variant_v<12>(a, epi, val, sms, s, launch);
+        case 13: return launch_variant_v<13>(a, epi, val, sms, s, launch);
+        case 14: return launch_variant_v<14>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
+}
+
+int spgemm_prepare(int epi, bool values, int sched, int force_accum) {
+    KArgs none{};
+    for (int v = 0; v < NV; ++v) {
+        cudaError_t e = launch_variant(v, none, epi, values, ctx().num_sms, nullptr, false);
+        if (e != cudaSuccess) return cuda_fail(e, "masked SpGEMM variant setup");
+    }
+    return sched_prepare(sched, force_accum);
+}
+
+size_t spgemm_scratch_bytes(int64_t m) {
+    auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, static_cast<int64_t *>(nullptr),
+                                  static_cast<int64_t *>(nullptr), m + 1);
+    return r(8 * m) + r(4 * m) + r(2 * m) + r(4 * m) + 2 * r(8 * (m + 1)) + r(sizeof(BinStats) * NBINS) +
+           r(4 * NBINS) + r(4 * (6 * NV + 4)) + r(4 * NV) + r(tmp_bytes);
 }
 
 // ---------------------------------------------------------------------------

@@ -16,7 +16,14 @@ graphkokkos_b200/csrc/gk_sched.cuh).  This module
 The model changes only which variant runs a bin; every variant computes the
 same integer terms, so results stay bit-exact.
 
+The same network (its outputs 0 and 1) also picks the forward-level shape of
+batched BC, pull or push (graphkokkos_b200/csrc/bc.cu): the BC sweep times
+every forward level of seeded runs both ways (gk_bc_tune) and the model is
+trained on log2 microseconds per level, saved as sched/bc_model.npz and handed
+to the library with gk_bc_set_model.
+
   python -m graphkokkos_b200.sched --train          # sweep the training graphs, train, save
+  python -m graphkokkos_b200.sched --train-bc       # the same for the BC level shapes
 """
 from __future__ import annotations
 
@@ -35,6 +42,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_DIR = os.path.join(HERE, "sched")
 MODEL_PATH = os.path.join(MODEL_DIR, "model.npz")
 DATA_PATH = os.path.join(MODEL_DIR, "sweep.npz")
+BC_MODEL_PATH = os.path.join(MODEL_DIR, "bc_model.npz")
+BC_DATA_PATH = os.path.join(MODEL_DIR, "bc_sweep.npz")
+BC_PULL, BC_PUSH = 0, 1
 
 MLP_H = 32
 
@@ -54,6 +64,13 @@ def model_size():
 def load_model(path=MODEL_PATH):
     w = np.ascontiguousarray(np.load(path)["w"], dtype=np.float32)
     check(_lib.load().gk_sched_set_model(w.ctypes.data, w.shape[0]))
+    return w
+
+
+def load_bc_model(path=BC_MODEL_PATH):
+    """Loads the learned BC forward-shape model (gk_bc_set_model)."""
+    w = np.ascontiguousarray(np.load(path)["w"], dtype=np.float32)
+    check(_lib.load().gk_bc_set_model(w.ctypes.data, w.shape[0]))
     return w
 
 
@@ -255,6 +272,102 @@ def load_dataset(path=DATA_PATH):
 
 
 # ---------------------------------------------------------------------------
+# batched BC: per-level forward shape (pull or push)
+# ---------------------------------------------------------------------------
+def bc_tune(A, sources, shape, max_levels=512):
+    """One BC run with every forward level on `shape` (0 pull, 1 push, -1 the
+    plain rule), levels driven from the host; returns (per-level ms, per-level
+    features, bc)."""
+    from . import api
+    lib = _lib.load()
+    nv, nf, nb = dims()
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.int32))
+    if A.is_cuda:
+        import torch
+        src = torch.as_tensor(src).to(A.rowptr.device)
+    out = api._empty_like_space(A.rowptr, (A.m,), np.float64)
+    ms = np.zeros(max_levels, dtype=np.float32)
+    feat = np.zeros((max_levels, nf), dtype=np.float32)
+    n = ctypes.c_int(0)
+    g = A.as_gk()
+    check(lib.gk_bc_tune(ctypes.byref(g), api._ptr(src), len(sources), int(shape), api._ptr(out), ms.ctypes.data,
+                         feat.ctypes.data, max_levels, ctypes.byref(n), _stream(A)))
+    k = min(n.value, max_levels)
+    return ms[:k].copy(), feat[:k].copy(), out
+
+
+def bc_plain_shape(f):
+    """The plain rule of the device (bc.cu, bc_plain_shape) from a level's features."""
+    nf_, ef, mu, m = (2.0 ** f[0] - 1, 2.0 ** f[1] - 1, 2.0 ** f[3] - 1, 2.0 ** f[4] - 1)
+    if ef * 14.0 < mu:
+        return BC_PUSH
+    if nf_ * 24.0 < m:
+        return BC_PUSH
+    return BC_PULL
+
+
+def bc_sweep(A, sources, name, reps=2, log=print):
+    """Times every forward level of a BC run as pull and as push (best of
+    reps); returns one record per level."""
+    best = {}
+    feats = None
+    for shape in (BC_PULL, BC_PUSH):
+        for _ in range(reps):
+            ms, f, _ = bc_tune(A, sources, shape)
+            if feats is None:
+                feats = f
+            t = best.setdefault(shape, ms.copy())
+            np.minimum(t, ms, out=t)
+    recs = []
+    for i in range(len(feats)):
+        ms = {BC_PULL: float(best[BC_PULL][i]), BC_PUSH: float(best[BC_PUSH][i])}
+        recs.append(dict(graph=name, level=i + 1, features=feats[i].tolist(), ms=ms,
+                         plain=bc_plain_shape(feats[i])))
+        log(f"  {name} level {i + 1:3d}  pull {ms[0]:8.3f} ms  push {ms[1]:8.3f} ms  plain "
+            f"{'push' if recs[-1]['plain'] else 'pull'}")
+    return recs
+
+
+def bc_dataset(recs):
+    nv, nf, nb = dims()
+    X = np.zeros((len(recs), nf), dtype=np.float32)
+    Y = np.zeros((len(recs), nv), dtype=np.float32)
+    M = np.zeros((len(recs), nv), dtype=np.float32)
+    for i, r in enumerate(recs):
+        X[i] = r["features"]
+        for v, ms in r["ms"].items():
+            Y[i, v] = np.log2(max(ms, 1e-4) * 1e3)  # log2 microseconds of the level
+            M[i, v] = 1.0
+    return X, Y, M
+
+
+def bc_choose(out):
+    return [BC_PUSH if o[BC_PUSH] < o[BC_PULL] else BC_PULL for o in out]
+
+
+def bc_evaluate(recs, picks):
+    plain = learned = best = 0.0
+    for r, p in zip(recs, picks):
+        ms = r["ms"]
+        plain += ms[r["plain"]]
+        learned += ms[p]
+        best += min(ms.values())
+    return dict(plain_ms=plain, learned_ms=learned, best_ms=best)
+
+
+def load_bc_dataset(path=BC_DATA_PATH):
+    recs = json.loads(str(np.load(path)["records"]))
+    for r in recs:
+        r["ms"] = {int(k): float(v) for k, v in r["ms"].items()}
+    return recs
+
+
+def bc_sources(m, n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.choice(m, size=min(n, m), replace=False)
+
+
+# ---------------------------------------------------------------------------
 # training graphs (seeds differ from the benchmark graphs')
 # ---------------------------------------------------------------------------
 TRAIN_GRAPHS = [
@@ -269,6 +382,17 @@ TRAIN_GRAPHS = [
 KTRUSS_GRAPHS = [
     ("rmat18-s18", dict(kind="rmat", scale=18, seed=18)),
     ("rmat20-s19", dict(kind="rmat", scale=20, seed=19)),
+]
+
+
+BC_GRAPHS = [
+    ("rmat16-s21-b512", dict(kind="rmat", scale=16, seed=21), 512, 31),
+    ("rmat18-s22-b512", dict(kind="rmat", scale=18, seed=22), 512, 32),
+    ("rmat18-s23-b128", dict(kind="rmat", scale=18, seed=23), 128, 33),
+    ("rmat19-s24-b512", dict(kind="rmat", scale=19, seed=24), 512, 34),
+    ("rmat20-s25-b256", dict(kind="rmat", scale=20, seed=25), 256, 35),
+    ("er256k-d16-s26-b512", dict(kind="er", n=1 << 18, nedges=1 << 21, seed=26), 512, 36),
+    ("er128k-d8-s27-b256", dict(kind="er", n=1 << 17, nedges=1 << 19, seed=27), 256, 37),
 ]
 
 
@@ -287,7 +411,11 @@ def main():
     ap.add_argument("--max-scale", type=int, default=24)
     ap.add_argument("--out", default=MODEL_DIR, help="directory for model.npz (and sweep.npz with --train)")
     ap.add_argument("--data", default=DATA_PATH, help="sweep to train from with --retrain")
+    ap.add_argument("--train-bc", action="store_true", help="sweep the BC graphs, train and save the BC model")
+    ap.add_argument("--retrain-bc", action="store_true", help="train the BC model from the saved BC sweep")
     args = ap.parse_args()
+    if args.train_bc or args.retrain_bc:
+        return main_bc(args)
     model_path = os.path.join(args.out, "model.npz")
     data_path = os.path.join(args.out, "sweep.npz") if args.train else args.data
     import torch
@@ -315,6 +443,28 @@ def main():
     w, trace = train(X, Y, M, epochs=args.epochs)
     picks = choose(forward_gpu(w, X), recs)
     ev = evaluate(recs, picks)
+    print(json.dumps({"samples": len(recs), "loss_first": float(trace[0]), "loss_last": float(trace[-1]), **ev}))
+    save_model(w, model_path, samples=len(recs), epochs=args.epochs, final_loss=float(trace[-1]), **ev)
+
+
+def main_bc(args):
+    import torch
+    torch.cuda.set_device(0)
+    model_path = os.path.join(args.out, "bc_model.npz")
+    data_path = os.path.join(args.out, "bc_sweep.npz") if args.train_bc else BC_DATA_PATH
+    if args.train_bc:
+        recs = []
+        for name, spec, nsrc, sseed in BC_GRAPHS:
+            A = build_graph(spec)
+            recs += bc_sweep(A, bc_sources(A.m, nsrc, sseed), name)
+            del A
+            torch.cuda.empty_cache()
+        save_dataset(recs, data_path)
+    recs = load_bc_dataset(data_path)
+    X, Y, M = bc_dataset(recs)
+    w, trace = train(X, Y, M, epochs=args.epochs)
+    picks = bc_choose(forward_gpu(w, X))
+    ev = bc_evaluate(recs, picks)
     print(json.dumps({"samples": len(recs), "loss_first": float(trace[0]), "loss_last": float(trace[-1]), **ev}))
     save_model(w, model_path, samples=len(recs), epochs=args.epochs, final_loss=float(trace[-1]), **ev)
 

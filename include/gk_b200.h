@@ -228,6 +228,24 @@ int gk_mlp_train(float *w, const float *X, const float *Y, const float *mask, in
                  float *loss_trace, void *stream);
 int gk_mlp_forward(const float *w, const float *X, int n, float *out, void *stream);
 
+/* Forward-level shape of batched BC (pull: vertices gather from their
+ * in-neighbours; push: frontier vertices scatter to their out-neighbours).
+ * GK_SCHED_PLAIN picks by the direction-optimising rule, GK_SCHED_LEARNED by
+ * an MLP of the same layout (gk_sched_model_size() floats) whose outputs 0 and
+ * 1 predict log2 microseconds of a pull and a push level, loaded here.  The
+ * shape changes only how the level is computed: sigma are integer path counts
+ * in FP64, exact in any order of addition. */
+int gk_bc_set_model(const float *weights, size_t n_floats);
+int gk_bc_has_model(void);
+
+/* Autotuning run of gk_bc_batch (at most 512 sources, one chunk) with every
+ * forward level on `shape` (0 pull, 1 push, -1 the plain rule), the levels
+ * driven from the host: level_ms[i] receives the CUDA-event time of forward
+ * level i+1 and level_feat[i*gk_sched_num_features()...] its features, for
+ * i < min(*nlevels, max_levels); bc as gk_bc_batch. */
+int gk_bc_tune(const gk_csr *A, const int32_t *sources, int nsources, int shape, double *bc, float *level_ms,
+               float *level_feat, int max_levels, int *nlevels, void *stream);
+
 /* ----- profiling (no reference counterpart; the reference prints chrono
  * brackets, src/main.cpp:74-86) -------------------------------------------------- */
 

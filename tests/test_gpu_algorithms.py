@@ -62,6 +62,28 @@ def test_ktruss_fixed_point(gk, cuda):
     assert it2 == 1 and T2.nnz == T.nnz
 
 
+def test_ktruss_graph_loop_matches_host_loop(gk, cuda):
+    """The pass loop runs as one CUDA graph (conditional while node); with
+    profiling on the host drives the same passes.  Both, and both schedulers,
+    give the same edge set and pass count."""
+    lib = gk.load()
+    A = gk.gen_rmat(13, 16, seed=4, device="cuda")
+    T, it = gk.ktruss(A, 5)
+    from graphkokkos_b200 import sched
+    sched.load_model()
+    TL, itL = gk.ktruss(A, 5, sched="learned")
+    lib.gk_prof_enable(1)
+    try:
+        TH, itH = gk.ktruss(A, 5)
+    finally:
+        lib.gk_prof_enable(0)
+    assert it == itL == itH and it > 2
+    for X in (TL, TH):
+        assert X.nnz == T.nnz
+        assert np.array_equal(X.rowptr.cpu().numpy(), T.rowptr.cpu().numpy())
+        assert np.array_equal(X.col.cpu().numpy(), T.col.cpu().numpy())
+
+
 # ---------------------------------------------------------------------------
 # betweenness centrality
 # ---------------------------------------------------------------------------
@@ -101,6 +123,42 @@ def test_bc_heavy_vertices(gk, orc, cuda):
     src = np.arange(0, 2000, 17)
     np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), rtol=BC_RTOL,
                                atol=1e-9)
+
+
+@pytest.mark.parametrize("shape", [0, 1, -1])
+def test_bc_forward_shapes_match_oracle(gk, orc, cuda, shape):
+    """Every forward level as pull (0), as push (1), or by the plain rule (-1),
+    driven from the host with per-level timing: same FP64 result."""
+    from graphkokkos_b200 import sched
+    cases = [(gk.gen_rmat(11, 16, seed=3), 200, 1),
+             (G.from_edges(2000, [(0, i) for i in range(1, 2000)] + [(i, i + 1) for i in range(1, 1999, 3)]), 90, 2),
+             (G.random_csr(300, 300, 0.02, seed=11), 40, 3)]
+    for A, nsrc, seed in cases:
+        src = np.random.default_rng(seed).choice(A.m, size=nsrc, replace=False)
+        ms, feat, bc = sched.bc_tune(dev(A), src, shape)
+        assert len(ms) >= 1 and np.all(ms > 0) and feat.shape == (len(ms), 8)
+        want = orc.bc_f64(A, src) if A.m != 300 else G.brandes_f64(A, src)
+        np.testing.assert_allclose(bc.cpu().numpy(), want, rtol=BC_RTOL, atol=1e-9)
+
+
+def test_bc_graph_loop_matches_host_loop(gk, cuda):
+    """The level loops run as CUDA graphs; with profiling on the host drives
+    the same levels.  Plain and learned shape choices agree too."""
+    from graphkokkos_b200 import sched
+    lib = gk.load()
+    A = gk.gen_rmat(13, 16, seed=6, device="cuda")
+    src = np.random.default_rng(6).choice(A.m, size=300, replace=False)
+    ref = gk.bc_batch(A, src).cpu().numpy()
+    lib.gk_prof_enable(2)
+    try:
+        host = gk.bc_batch(A, src).cpu().numpy()
+    finally:
+        lib.gk_prof_enable(0)
+    np.testing.assert_allclose(host, ref, rtol=BC_RTOL, atol=1e-9)
+    if os.path.exists(sched.BC_MODEL_PATH):
+        sched.load_bc_model()
+        learned = gk.bc_batch(A, src, sched="learned").cpu().numpy()
+        np.testing.assert_allclose(learned, ref, rtol=BC_RTOL, atol=1e-9)
 
 
 def test_bc_golden(gk, cuda):
