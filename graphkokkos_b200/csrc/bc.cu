@@ -27,7 +27,10 @@
 // rule is an MLP over the level's frontier statistics, trained on measured
 // per-level times of both shapes.  Backward levels pull: one warp per vertex
 // of level d, lanes testing 32 successors' level-(d+1) words at a time.
-// Vertices with more than BC_HEAVY neighbours are handled by a whole CTA.
+// Vertices with more than BC_HEAVY neighbours have their neighbour lists cut
+// into items of BC_ITEM_EDGES edges, one CTA each, so that a hub no longer
+// holds one CTA for the whole level; the items' partial sums are added per
+// vertex in item order.
 // R(v,s) = (1+delta)/sigma replaces the reference's Nspinv∘Bcu; delta is summed
 // into bc[v] as soon as it is final, in a fixed order (deterministic).
 //
@@ -35,6 +38,8 @@
 // so the level loops are CUDA graphs: a conditional while node around one
 // captured level, the condition set by the level's last kernel.  Both forward
 // shapes are launched every level and the one not chosen returns at once.
+#include <cub/cub.cuh>
+
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -47,11 +52,31 @@ namespace gk {
 
 int transpose_device(const DevCsr &A, int64_t *orp, int32_t *ocol, int32_t *oval, cudaStream_t s, Scratch &scr);
 
+// Widest chunk: 32 * GK_BC_TMAX sources (a power of two, at most 16).
+#ifndef GK_BC_TMAX
+#define GK_BC_TMAX 16
+#endif
+// Resident CTAs per SM the light level kernels are register-capped for.
+#ifndef GK_BC_MINB
+#define GK_BC_MINB 2
+#endif
 constexpr int BC_HEAVY = 512;
 constexpr int BC_NW_HEAVY = 8;  // T=16: 8*16*32 doubles = 32 KB of static shared memory
 constexpr int BC_PULL = 0, BC_PUSH = 1;
 constexpr int BC_LEVEL_BATCH = 16;  // level bitmaps allocated at a time
 constexpr int BC_FEAT = NFEAT;
+constexpr int BC_ITEM_EDGES = 2048;  // edges of a heavy vertex per CTA work item
+
+// Vertices with more than BC_HEAVY neighbours, their neighbour lists cut
+// into items of BC_ITEM_EDGES edges (one CTA each).  Pull-type items write
+// per-item partial sums; a warp per heavy vertex adds its items' partials in
+// item order (deterministic) and emits.
+struct HeavySet {
+    const int32_t *list;   // heavy vertices
+    const int32_t *first;  // items of list[h]: first[h] .. first[h+1]-1
+    const int32_t *item_h; // heavy index of each item
+    int n, items;
+};
 
 // learned forward-shape model (same network as the row-bin scheduler's;
 // outputs 0 and 1 predict log2 microseconds of a pull and a push level)
@@ -73,7 +98,17 @@ struct BcState {
     unsigned long long nn, en, bn;  // F_{d+1} under construction
     unsigned long long visited;     // (vertex, source) pairs reached, sources included
     unsigned long long pushes, pulls;
+    unsigned long long cur_pull, cur_push, cur_bwd;  // vertex cursors of the light kernels
 };
+
+// Light kernels hand vertices to warps BC_GRAB at a time from a counter, so
+// that a warp which met expensive vertices does not hold the level back.
+constexpr int BC_GRAB = 16;
+__device__ __forceinline__ int64_t grab_vertices(unsigned long long *cursor, int lane) {
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(cursor, static_cast<unsigned long long>(BC_GRAB));
+    return static_cast<int64_t>(__shfl_sync(0xFFFFFFFFu, b, 0));
+}
 
 template <int T>
 __device__ __forceinline__ void load_words(const uint32_t *p, uint32_t (&w)[T]) {
@@ -264,16 +299,16 @@ __device__ __forceinline__ int pull_emit(int64_t i, int W, int lane, const uint3
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) k_bc_pull(DevCsr AT, DevCsr A, BcState *st, uint32_t *V, double *sigma,
-                                                 int W, const uint32_t *act) {
+__global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_pull(DevCsr AT, DevCsr A, BcState *st, uint32_t *V,
+                                                             double *sigma, int W, const uint32_t *act) {
     if (st->mode != BC_PULL) return;
     const int d = st->d;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     unsigned long long n = 0, e = 0, b = 0;
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < AT.m; i += warps) {
+    for (int64_t base = grab_vertices(&st->cur_pull, lane); base < AT.m; base = grab_vertices(&st->cur_pull, lane))
+    for (int64_t i = base, iend = min(base + BC_GRAB, AT.m); i < iend; ++i) {
         const int64_t e0 = AT.rp[i], e1 = AT.rp[i + 1];
         if (e0 == e1 || e1 - e0 > BC_HEAVY) continue;
         uint32_t vis[T], need[T];
@@ -299,20 +334,35 @@ __global__ void __launch_bounds__(256) k_bc_pull(DevCsr AT, DevCsr A, BcState *s
     add_level_stats(n, e, b, &st->nn);
 }
 
+// Reduces the NW warps' T x 32 partial sums of a CTA into warp 0's acc.
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_heavy(DevCsr AT, DevCsr A, const int32_t *heavy,
-                                                                    int nheavy, BcState *st, uint32_t *V,
-                                                                    double *sigma, int W, const uint32_t *act) {
+__device__ __forceinline__ void cta_reduce(double (&acc)[T], double (*part)[T][32], int warp, int lane) {
+#pragma unroll
+    for (int t = 0; t < T; ++t) part[warp][t][lane] = acc[t];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            double sum = 0.0;
+            for (int w = 0; w < BC_NW_HEAVY; ++w) sum += part[w][t][lane];
+            acc[t] = sum;
+        }
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_items(DevCsr AT, HeavySet hs, BcState *st,
+                                                                    const uint32_t *V, const double *sigma, int W,
+                                                                    const uint32_t *act, double *partials) {
     if (st->mode != BC_PULL) return;
     __shared__ double part[BC_NW_HEAVY][T][32];
-    const int d = st->d;
-    const uint32_t *__restrict__ Fd = st->fptr[d];
-    uint32_t *Fn = st->fptr[d + 1];
+    const uint32_t *__restrict__ Fd = st->fptr[st->d];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long n = 0, e = 0, b = 0;
-    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
-        const int64_t i = heavy[h];
-        const int64_t e0 = AT.rp[i], e1 = AT.rp[i + 1];
+    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+        const int h = hs.item_h[it];
+        const int64_t i = hs.list[h];
+        const int64_t e0 = AT.rp[i] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
+        const int64_t e1 = min(AT.rp[i + 1], e0 + BC_ITEM_EDGES);
         uint32_t vis[T], need[T];
         load_words<T>(V + i * T, vis);
         uint32_t open = 0;
@@ -321,29 +371,50 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_heavy(DevCsr AT, D
             need[t] = ~vis[t] & act[t];
             open |= need[t];
         }
-        if (!open) continue;  // uniform across the CTA
+        if (!open) continue;  // uniform across the CTA (the emit kernel skips the vertex too)
         double acc[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
         pull_sigma<T>(AT, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fd, need, sigma, W, lane, acc);
-#pragma unroll
-        for (int t = 0; t < T; ++t) part[warp][t][lane] = acc[t];
-        __syncthreads();
+        cta_reduce<T>(acc, part, warp, lane);
         if (warp == 0) {
 #pragma unroll
-            for (int t = 0; t < T; ++t) {
-                double sum = 0.0;
-                for (int w = 0; w < BC_NW_HEAVY; ++w) sum += part[w][t][lane];
-                acc[t] = sum;
-            }
-            const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
-            if (c && lane == 0) {
-                ++n;
-                e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
-                b += c;
-            }
+            for (int t = 0; t < T; ++t) partials[(int64_t)it * W + 32 * t + lane] = acc[t];
         }
         __syncthreads();
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(256) k_bc_pull_heavy_emit(DevCsr A, HeavySet hs, BcState *st, uint32_t *V,
+                                                            double *sigma, int W, const uint32_t *act,
+                                                            const double *partials) {
+    if (st->mode != BC_PULL) return;
+    uint32_t *Fn = st->fptr[st->d + 1];
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    unsigned long long n = 0, e = 0, b = 0;
+    for (int h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < hs.n; h += warps) {
+        const int64_t i = hs.list[h];
+        uint32_t vis[T];
+        load_words<T>(V + i * T, vis);
+        uint32_t open = 0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) open |= ~vis[t] & act[t];
+        if (!open) continue;
+        double acc[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) acc[t] = 0.0;
+        for (int it = hs.first[h]; it < hs.first[h + 1]; ++it) {
+#pragma unroll
+            for (int t = 0; t < T; ++t) acc[t] += partials[(int64_t)it * W + 32 * t + lane];
+        }
+        const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
+        if (c && lane == 0) {
+            ++n;
+            e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
+            b += c;
+        }
     }
     add_level_stats(n, e, b, &st->nn);
 }
@@ -406,14 +477,14 @@ __device__ __forceinline__ bool push_source(int64_t u, const uint32_t *__restric
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) k_bc_push(DevCsr A, BcState *st, const uint32_t *V, double *sigma, int W) {
+__global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_push(DevCsr A, BcState *st, const uint32_t *V, double *sigma, int W) {
     if (st->mode != BC_PUSH) return;
     const int d = st->d;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t u = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < A.m; u += warps) {
+    for (int64_t base = grab_vertices(&st->cur_push, lane); base < A.m; base = grab_vertices(&st->cur_push, lane))
+    for (int64_t u = base, uend = min(base + BC_GRAB, A.m); u < uend; ++u) {
         const int64_t e0 = A.rp[u], e1 = A.rp[u + 1];
         if (e0 == e1 || e1 - e0 > BC_HEAVY) continue;
         uint32_t fu[T];
@@ -424,20 +495,22 @@ __global__ void __launch_bounds__(256) k_bc_push(DevCsr A, BcState *st, const ui
 }
 
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_push_heavy(DevCsr A, const int32_t *heavy, int nheavy,
-                                                                    BcState *st, const uint32_t *V, double *sigma,
-                                                                    int W) {
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_push_items(DevCsr A, HeavySet hs, BcState *st,
+                                                                    const uint32_t *V, double *sigma, int W) {
     if (st->mode != BC_PUSH) return;
     const int d = st->d;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
-        const int64_t u = heavy[h];
+    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+        const int h = hs.item_h[it];
+        const int64_t u = hs.list[h];
+        const int64_t e0 = A.rp[u] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
+        const int64_t e1 = min(A.rp[u + 1], e0 + BC_ITEM_EDGES);
         uint32_t fu[T];
         double su[T];
         if (!push_source<T>(u, Fd, sigma, W, lane, fu, su)) continue;
-        push_sigma<T>(A, A.rp[u] + 32 * warp, A.rp[u + 1], 32 * BC_NW_HEAVY, fu, su, V, sigma, Fn, W, T, lane);
+        push_sigma<T>(A, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, fu, su, V, sigma, Fn, W, T, lane);
     }
 }
 
@@ -481,6 +554,7 @@ __global__ void k_bc_fwd_end(BcState *st, int64_t max_depth, cudaGraphConditiona
         more = (st->d + 1 <= st->levels && st->d < max_depth) ? 1 : 0;
     }
     st->nn = st->en = st->bn = 0;
+    st->cur_pull = st->cur_push = 0;
     if (in_graph) cudaGraphSetConditional(h, static_cast<unsigned>(more));
 }
 
@@ -555,14 +629,14 @@ __device__ __forceinline__ void bwd_emit(int64_t v, int W, int lane, const uint3
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) k_bc_backward(DevCsr A, const BcState *st, const double *sigma, double *R,
-                                                     int W, double *bc) {
+__global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcState *st, const double *sigma,
+                                                                 double *R, int W, double *bc) {
     const int d = st->bd;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < A.m; v += warps) {
+    for (int64_t base = grab_vertices(&st->cur_bwd, lane); base < A.m; base = grab_vertices(&st->cur_bwd, lane))
+    for (int64_t v = base, vend = min(base + BC_GRAB, A.m); v < vend; ++v) {
         const int64_t e0 = A.rp[v], e1 = A.rp[v + 1];
         if (e1 - e0 > BC_HEAVY) continue;
         uint32_t fv[T];
@@ -580,16 +654,18 @@ __global__ void __launch_bounds__(256) k_bc_backward(DevCsr A, const BcState *st
 }
 
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_heavy(DevCsr A, const int32_t *heavy, int nheavy,
-                                                                       const BcState *st, const double *sigma,
-                                                                       double *R, int W, double *bc) {
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_items(DevCsr A, HeavySet hs, const BcState *st,
+                                                                        const double *R, int W, double *partials) {
     __shared__ double part[BC_NW_HEAVY][T][32];
     const int d = st->bd;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int h = blockIdx.x; h < nheavy; h += gridDim.x) {
-        const int64_t v = heavy[h];
+    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+        const int h = hs.item_h[it];
+        const int64_t v = hs.list[h];
+        const int64_t e0 = A.rp[v] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
+        const int64_t e1 = min(A.rp[v + 1], e0 + BC_ITEM_EDGES);
         uint32_t fv[T];
         load_words<T>(Fd + v * T, fv);
         uint32_t any = 0;
@@ -599,25 +675,45 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_heavy(DevCsr A
         double sum[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
-        pull_r<T>(A, A.rp[v] + 32 * warp, A.rp[v + 1], 32 * BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
-#pragma unroll
-        for (int t = 0; t < T; ++t) part[warp][t][lane] = sum[t];
-        __syncthreads();
+        pull_r<T>(A, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
+        cta_reduce<T>(sum, part, warp, lane);
         if (warp == 0) {
 #pragma unroll
-            for (int t = 0; t < T; ++t) {
-                double x = 0.0;
-                for (int w = 0; w < BC_NW_HEAVY; ++w) x += part[w][t][lane];
-                sum[t] = x;
-            }
-            bwd_emit<T>(v, W, lane, fv, sum, sigma, R, bc);
+            for (int t = 0; t < T; ++t) partials[(int64_t)it * W + 32 * t + lane] = sum[t];
         }
         __syncthreads();
     }
 }
 
+template <int T>
+__global__ void __launch_bounds__(256) k_bc_backward_heavy_emit(HeavySet hs, const BcState *st, const double *sigma,
+                                                                double *R, int W, double *bc,
+                                                                const double *partials) {
+    const uint32_t *__restrict__ Fd = st->fptr[st->bd];
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < hs.n; h += warps) {
+        const int64_t v = hs.list[h];
+        uint32_t fv[T];
+        load_words<T>(Fd + v * T, fv);
+        uint32_t any = 0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) any |= fv[t];
+        if (!any) continue;
+        double sum[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) sum[t] = 0.0;
+        for (int it = hs.first[h]; it < hs.first[h + 1]; ++it) {
+#pragma unroll
+            for (int t = 0; t < T; ++t) sum[t] += partials[(int64_t)it * W + 32 * t + lane];
+        }
+        bwd_emit<T>(v, W, lane, fv, sum, sigma, R, bc);
+    }
+}
+
 __global__ void k_bc_bwd_end(BcState *st, cudaGraphConditionalHandle h, int in_graph) {
     st->bd -= 1;
+    st->cur_bwd = 0;
     if (in_graph) cudaGraphSetConditional(h, st->bd >= 1 ? 1u : 0u);
 }
 
@@ -627,13 +723,24 @@ __global__ void k_heavy_list(DevCsr A, int32_t *list, int *count) {
         if (A.rp[i + 1] - A.rp[i] > BC_HEAVY) list[atomicAdd(count, 1)] = static_cast<int32_t>(i);
 }
 
+__global__ void k_heavy_item_counts(DevCsr A, const int32_t *list, int n, int32_t *cnt) {
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x) {
+        const int64_t v = list[h];
+        cnt[h] = static_cast<int32_t>((A.rp[v + 1] - A.rp[v] + BC_ITEM_EDGES - 1) / BC_ITEM_EDGES);
+    }
+}
+
+__global__ void k_heavy_items(const int32_t *first, int n, int32_t *item_h) {
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < n; h += gridDim.x * blockDim.x)
+        for (int it = first[h]; it < first[h + 1]; ++it) item_h[it] = h;
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 struct BcBuffers {
     DevCsr A, AT;
-    int32_t *heavyA, *heavyAT;
-    int nheavyA, nheavyAT;
+    HeavySet hA, hAT;  // heavy vertices of A (push, backward) and of AT (pull)
 };
 
 // Options of a BC run: scheduler, a forced forward shape (autotuning), and
@@ -725,6 +832,11 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
     GK_CHECK(local.alloc(&act, T));
     GK_CHECK(local.alloc(&st, 1));
     if (opt.level_feat && opt.log_cap > 0) GK_CHECK(local.alloc(&feat_dev, (size_t)opt.log_cap * BC_FEAT));
+    double *partials;  // per heavy item: W partial sums
+    {
+        const int items = g.hA.items > g.hAT.items ? g.hA.items : g.hAT.items;
+        GK_CHECK(local.alloc(&partials, (size_t)(items > 0 ? items : 1) * W));
+    }
     GK_CUDA(cudaMemsetAsync(V, 0, sizeof(uint32_t) * m * T, s));
     GK_CUDA(cudaMemsetAsync(sigma, 0, sizeof(double) * m * W, s));  // push levels add into it
     GK_CUDA(cudaMemsetAsync(st, 0, sizeof(BcState), s));
@@ -790,16 +902,20 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
         auto fwd_level = [&](cudaStream_t ls, cudaGraphConditionalHandle h, bool in_graph) {
             k_bc_choose<<<1, 1, 0, ls>>>(st, opt.force, opt.sched, m, nnz, W, feat_dev, opt.log_cap);
             k_bc_pull<T><<<sms * 8, 256, 0, ls>>>(g.AT, g.A, st, V, sigma, W, act);
-            if (g.nheavyAT)
-                k_bc_pull_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.AT, g.A, g.heavyAT, g.nheavyAT, st, V,
-                                                                       sigma, W, act);
+            int k = 0;
+            if (g.hAT.n) {
+                k_bc_pull_items<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.AT, g.hAT, st, V, sigma, W, act, partials);
+                k_bc_pull_heavy_emit<T><<<sms, 256, 0, ls>>>(g.A, g.hAT, st, V, sigma, W, act, partials);
+                k += 2;
+            }
             k_bc_push<T><<<sms * 8, 256, 0, ls>>>(g.A, st, V, sigma, W);
-            if (g.nheavyA)
-                k_bc_push_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.heavyA, g.nheavyA, st, V, sigma,
-                                                                       W);
+            if (g.hA.n) {
+                k_bc_push_items<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.hA, st, V, sigma, W);
+                k += 1;
+            }
             k_bc_push_finish<T><<<sms * 4, 256, 0, ls>>>(g.A, st, V);
             k_bc_fwd_end<<<1, 1, 0, ls>>>(st, m, h, in_graph ? 1 : 0);
-            return 5 + (g.nheavyAT ? 1 : 0) + (g.nheavyA ? 1 : 0);
+            return 5 + k;
         };
         BcState hs{};
         bool graph_ok = !opt.host_loop && !prof_any();
@@ -885,11 +1001,14 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
         }
         auto bwd_level = [&](cudaStream_t ls, cudaGraphConditionalHandle h, bool in_graph) {
             k_bc_backward<T><<<sms * 8, 256, 0, ls>>>(g.A, st, sigma, R, W, bc);
-            if (g.nheavyA)
-                k_bc_backward_heavy<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.heavyA, g.nheavyA, st, sigma, R,
-                                                                           W, bc);
+            int k = 0;
+            if (g.hA.n) {
+                k_bc_backward_items<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.hA, st, R, W, partials);
+                k_bc_backward_heavy_emit<T><<<sms, 256, 0, ls>>>(g.hA, st, sigma, R, W, bc, partials);
+                k += 2;
+            }
             k_bc_bwd_end<<<1, 1, 0, ls>>>(st, h, in_graph ? 1 : 0);
-            return 2 + (g.nheavyA ? 1 : 0);
+            return 2 + k;
         };
         bool bgraph = !opt.host_loop && !prof_any();
         LevelGraph bg;
@@ -936,6 +1055,48 @@ static int ensure_bc_model(int sched) {
     return GK_OK;
 }
 
+// Heavy vertices of G and their work items (synchronises once for the counts).
+static int heavy_set(const DevCsr &G, HeavySet *hs, cudaStream_t s, Scratch &scr) {
+    const int sms = ctx().num_sms;
+    int32_t *list, *cnt, *first, *item_h;
+    int *n_dev;
+    GK_CHECK(scr.alloc(&list, G.m > 0 ? G.m : 1));
+    GK_CHECK(scr.alloc(&n_dev, 1));
+    GK_CUDA(cudaMemsetAsync(n_dev, 0, sizeof(int), s));
+    k_heavy_list<<<sms * 4, 256, 0, s>>>(G, list, n_dev);
+    int n = 0;
+    GK_CUDA(cudaMemcpyAsync(&n, n_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GK_CUDA(cudaStreamSynchronize(s));
+    note_launches(1);
+    hs->list = list;
+    hs->n = n;
+    hs->items = 0;
+    GK_CHECK(scr.alloc(&cnt, n + 1));
+    GK_CHECK(scr.alloc(&first, n + 1));
+    GK_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int32_t), s));
+    if (n > 0) {
+        k_heavy_item_counts<<<ceil_div(n, 256), 256, 0, s>>>(G, list, n, cnt);
+        note_launches(1);
+    }
+    size_t tb = 0;
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, first, n + 1, s));
+    void *tmp;
+    GK_CHECK(scr.alloc(reinterpret_cast<char **>(&tmp), tb));
+    GK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, first, n + 1, s));
+    int items = 0;
+    GK_CUDA(cudaMemcpyAsync(&items, first + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GK_CUDA(cudaStreamSynchronize(s));
+    GK_CHECK(scr.alloc(&item_h, items > 0 ? items : 1));
+    if (n > 0) {
+        k_heavy_items<<<ceil_div(n, 256), 256, 0, s>>>(first, n, item_h);
+        note_launches(1);
+    }
+    hs->first = first;
+    hs->item_h = item_h;
+    hs->items = items;
+    return GK_OK;
+}
+
 int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const BcOptions &opt, cudaStream_t s,
               Scratch &scr) {
     if (opt.sched != GK_SCHED_PLAIN && opt.sched != GK_SCHED_LEARNED) return fail(GK_ERR_ARG, "unknown scheduler mode");
@@ -950,26 +1111,14 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const B
     if (A.val) GK_CHECK(scr.alloc(&tval, A.nnz > 0 ? A.nnz : 1));
     GK_CHECK(transpose_device(A, trp, tcol, tval, s, scr));
     g.AT = DevCsr{A.m, A.m, A.nnz, trp, tcol, tval};
-    int *cnt;
-    GK_CHECK(scr.alloc(&g.heavyA, A.m > 0 ? A.m : 1));
-    GK_CHECK(scr.alloc(&g.heavyAT, A.m > 0 ? A.m : 1));
-    GK_CHECK(scr.alloc(&cnt, 2));
-    GK_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), s));
-    k_heavy_list<<<sms * 4, 256, 0, s>>>(g.A, g.heavyA, cnt);
-    note_launches(1);
-    k_heavy_list<<<sms * 4, 256, 0, s>>>(g.AT, g.heavyAT, cnt + 1);
-    note_launches(1);
-    int hc[2];
-    GK_CUDA(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
-    GK_CUDA(cudaStreamSynchronize(s));
-    g.nheavyA = hc[0];
-    g.nheavyAT = hc[1];
+    GK_CHECK(heavy_set(g.A, &g.hA, s, scr));
+    GK_CHECK(heavy_set(g.AT, &g.hAT, s, scr));
     GK_CUDA(cudaMemsetAsync(bc, 0, sizeof(double) * A.m, s));
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     for (int done = 0; done < nsrc;) {
         const int left = nsrc - done;
-        int T = 16;
+        int T = GK_BC_TMAX;
         while (T > 1 && 32 * (T / 2) >= left) T /= 2;
         // two FP64 m x W arrays must fit comfortably
         while (T > 1 && (double)A.m * 32 * T * 16 > 0.6 * (double)free_b) T /= 2;
