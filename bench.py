@@ -41,6 +41,7 @@ WORKLOADS = {
     "tc14": dict(kind="tc", scale=14, seed=1),
     "ktruss20": dict(kind="ktruss", scale=20, seed=2, k=5),
     "bc18": dict(kind="bc", scale=18, seed=3, nsrc=512, src_seed=4),
+    "tcbatch": dict(kind="tcbatch", ngraphs=4096, seed0=100),
 }
 
 
@@ -140,14 +141,17 @@ def time_steps(torch, fn, steps, warmup, dist=None):
     return e0.elapsed_time(e1) / steps
 
 
-def tc_roofline(gk, torch, L, sched, peak, peak_kind):
+def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None):
     """Per-variant CUDA-event durations of one profiled call (work totals)
     plus events-only brackets over timed calls; the dominant variant's
-    algorithmic bytes per launch divided by its mean launch time."""
+    algorithmic bytes per launch divided by its mean launch time.  `call`
+    runs the product (default: gk_tc_count on L into a device counter)."""
     lib = gk.load()
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    if call is None:
+        call = lambda: gk.tc_count_device(L, out, sched=sched)  # noqa: E731
     lib.gk_prof_enable(1)
-    gk.tc_count_device(L, out, sched=sched)
+    call()
     torch.cuda.synchronize()
     work = {}
     rec = gk._lib.GkProfRec()
@@ -156,7 +160,7 @@ def tc_roofline(gk, torch, L, sched, peak, peak_kind):
         work[rec.variant] = (rec.rows, rec.sum_a, rec.sum_m, rec.sum_work)
     lib.gk_prof_enable(2)
     for _ in range(3):
-        gk.tc_count_device(L, out, sched=sched)
+        call()
     lib.gk_prof_flush()
     times = {}
     for i in range(lib.gk_prof_count()):
@@ -486,6 +490,98 @@ def run_bc(args, wl, torch, gk, dist, rank, world):
     return line
 
 
+def build_batch(gk, torch, specs):
+    Ls = []
+    for spec in specs:
+        A = gk.api.gen_spec(spec)
+        L = gk.extract_lower(A)
+        L.col = L.col[:L.nnz].clone()
+        Ls.append(L)
+        del A
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return Ls
+
+
+def run_tcbatch(args, wl, torch, gk, dist, rank, world):
+    specs = gk.api.uneven_batch_specs(wl["ngraphs"], wl["seed0"])
+    Ls = build_batch(gk, torch, specs)
+    nnz = sum(L.nnz for L in Ls)
+    have_model = load_model(gk)
+    scheds = ["plain"] + (["learned"] if have_model else [])
+    lib = gk.load()
+    res = {}
+    ref = None
+    for sched in scheds:
+        out = [None]
+
+        def fn():
+            out[0] = gk.tc_count_batched(Ls, sched=sched)
+        if sched == scheds[-1]:
+            clocks = ClockSampler(torch.cuda.current_device())
+            clocks.start()
+            l0 = lib.gk_launch_count()
+        ms = time_steps(torch, fn, args.steps, args.warmup, dist)
+        if sched == scheds[-1]:
+            launches = (lib.gk_launch_count() - l0) // (args.steps + args.warmup)
+            clk = clocks.stop()
+        assert ref is None or np.array_equal(out[0], ref), "schedulers disagree"
+        ref = out[0]
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res[sched] = {"value": nnz * world / (ms_max / 1e3), "ms_per_step": ms_max}
+    head = scheds[-1]
+    line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic: seeded Erdos-Renyi and RMAT graphs generated on the device",
+            "config": {"workload": f"many-graph triangle counting, {len(Ls)} graphs (half ER, half RMAT-10..17), "
+                                   f"seeds {wl['seed0']}..{wl['seed0'] + len(Ls) - 1}, one batched call",
+                       "graphs": len(Ls), "nnz_lower_total": nnz, "vertices_total": sum(L.m for L in Ls),
+                       "sched": head, "triangles_total": int(ref.sum()),
+                       "l2": f"inputs larger than L2 ({nnz * 4 / 1e9:.2f} GB of columns)"},
+            "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        line["roofline"] = tc_roofline(gk, torch, None, head, peak, peak_kind,
+                                       call=lambda: gk.tc_count_batched(Ls, sched=head))
+        line["roofline"]["traffic"] = None
+        # end to end with host arrays: every graph's CSR copied in, counts read back
+        Hs = [L.to("cpu") for L in Ls]
+        for H in Hs:
+            H.rowptr = H.rowptr.pin_memory()
+            H.col = H.col.pin_memory()
+        gk.tc_count_batched(Hs, sched=head)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        got = gk.tc_count_batched(Hs, sched=head)
+        e2e_s = time.perf_counter() - t0
+        assert np.array_equal(got, ref)
+        line["e2e"] = {"value": nnz / e2e_s, "unit": "edges/s", "ms_per_step": e2e_s * 1e3,
+                       "h2d_bytes_per_step": sum(8 * (L.m + 1) + 4 * L.nnz for L in Ls),
+                       "d2h_bytes_per_step": 8 * len(Ls), "api": "gk_tc_count_batched with pinned host CSR arrays"}
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            kind = "reference" if oracle.ref_available() else "port"
+            sample = list(range(0, len(Ls), max(1, len(Ls) // 64)))
+            done_nz, sec, thr = 0, 0.0, 1
+            for g in sample:
+                Lh = Hs[g].numpy()
+                cnt, nz, s_, thr = oracle.tc_row_stride(Lh, 1, 0, kind=kind)
+                assert cnt == int(ref[g]), f"graph {g}: CPU count {cnt} != GPU {int(ref[g])}"
+                done_nz += nz
+                sec += s_
+                if sec > 20.0:
+                    break
+            line["cpu_baseline"] = {"value": done_nz / sec if sec > 0 else None, "unit": "edges/s", "cores": thr,
+                                    "kind": kind, "sample": f"whole graphs {sample[0]}, {sample[1] if len(sample) > 1 else ''}"
+                                    f", ... (every {max(1, len(Ls) // 64)}th graph, {done_nz} L entries, {sec:.1f} s), "
+                                    "counts checked against the GPU's"}
+    return line
+
+
 def main_ours(args):
     import torch
     rank, local, world = rank_info()
@@ -501,7 +597,7 @@ def main_ours(args):
     import graphkokkos_b200 as gk
     gk.load()
     wl = WORKLOADS[args.workload]
-    runner = {"tc": run_tc, "ktruss": run_ktruss, "bc": run_bc}[wl["kind"]]
+    runner = {"tc": run_tc, "ktruss": run_ktruss, "bc": run_bc, "tcbatch": run_tcbatch}[wl["kind"]]
     line = runner(args, wl, torch, gk, dist, rank, world)
     if rank == 0:
         print(json.dumps(line), flush=True)

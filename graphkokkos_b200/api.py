@@ -262,6 +262,46 @@ def gen_rmat(scale, edge_factor=16, seed=1, abc=RMAT_ABC, device="cpu") -> Csr:
     return Csr(m, m, rp, col[:nnz.value], None, int(nnz.value))
 
 
+def uneven_batch_specs(ngraphs, seed0):
+    """Parameters of an uneven many-graph batch: the first half Erdos-Renyi
+    G(n, M) with n log-uniform in [1e3, 1e5] and average degree uniform in
+    [4, 64] (M = n*d/2 sampled pairs), the second half RMAT with scale uniform
+    in [10, 17] and edge factor 16.  Graph g has seed seed0 + g, which also
+    draws its parameters.  Returns (kind, a, b, seed) tuples: ("er", n, M, seed)
+    or ("rmat", scale, edge_factor, seed)."""
+    specs = []
+    for g in range(ngraphs):
+        seed = seed0 + g
+        rng = np.random.default_rng(seed)
+        if g < ngraphs // 2:
+            n = int(round(10 ** rng.uniform(3.0, 5.0)))
+            d = float(rng.uniform(4.0, 64.0))
+            specs.append(("er", n, max(1, int(n * d / 2)), seed))
+        else:
+            specs.append(("rmat", int(rng.integers(10, 18)), 16, seed))
+    return specs
+
+
+def gen_spec(spec, device="cuda") -> Csr:
+    kind, a, b, seed = spec
+    return gen_rmat(a, b, seed=seed, device=device) if kind == "rmat" else gen_er(a, b, seed=seed, device=device)
+
+
+def disjoint_union(graphs: Sequence[Csr]) -> Csr:
+    """Block-diagonal CSR of several square graphs (device tensors)."""
+    import torch
+    rps, cols = [], []
+    vbase, ebase = 0, 0
+    for G in graphs:
+        rps.append(G.rowptr[:-1] + ebase)
+        cols.append(G.col[:G.nnz] + vbase)
+        vbase += G.m
+        ebase += G.nnz
+    dev = graphs[0].rowptr.device
+    rps.append(torch.tensor([ebase], dtype=torch.int64, device=dev))
+    return Csr(vbase, vbase, torch.cat(rps), torch.cat(cols), None, ebase)
+
+
 def gen_er(n, nedges, seed=1, device="cpu") -> Csr:
     lib = _lib.load()
     if device == "cpu":

@@ -378,6 +378,7 @@ TRAIN_GRAPHS = [
     ("rmat24-s15", dict(kind="rmat", scale=24, seed=15)),
     ("er1m-d16-s16", dict(kind="er", n=1 << 20, nedges=8 << 20, seed=16)),
     ("er4m-d32-s17", dict(kind="er", n=1 << 22, nedges=64 << 20, seed=17)),
+    ("batch512-s5000", dict(kind="batch", ngraphs=512, seed0=5000)),
 ]
 KTRUSS_GRAPHS = [
     ("rmat18-s18", dict(kind="rmat", scale=18, seed=18)),
@@ -398,6 +399,8 @@ BC_GRAPHS = [
 
 def build_graph(spec):
     from . import api
+    if spec["kind"] == "batch":  # an uneven many-graph batch as one block-diagonal graph
+        return api.disjoint_union([api.gen_spec(g) for g in api.uneven_batch_specs(spec["ngraphs"], spec["seed0"])])
     if spec["kind"] == "rmat":
         return api.gen_rmat(spec["scale"], 16, seed=spec["seed"], device="cuda")
     return api.gen_er(spec["n"], spec["nedges"], seed=spec["seed"], device="cuda")
