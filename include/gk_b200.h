@@ -134,7 +134,9 @@ int gk_ktruss(gk_csr_mut *inout, int k, int *iters, int sched, void *stream);
  * bc[v] = sum over sources s of Brandes' dependency delta_s(v), unnormalised,
  * as betweenness_centrality_batch (include/betweenness_centrality.h:406-506)
  * computes for sources 0..b-1 (:445-447).  A must be square.  bc has A.m
- * entries.  Sources must be distinct vertices. */
+ * entries.  Sources must be distinct vertices.  sched picks each forward
+ * level's kernel shape (pull or push): GK_SCHED_PLAIN by the direction-
+ * optimising rule, GK_SCHED_LEARNED by the model of gk_bc_set_model. */
 int gk_bc_batch(const gk_csr *A, const int32_t *sources, int nsources, double *bc, int sched,
                 void *stream);
 
