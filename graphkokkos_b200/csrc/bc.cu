@@ -224,9 +224,12 @@ __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_
     if (force >= 0) {
         mode = force;
     } else if (sched == GK_SCHED_LEARNED) {
+        // the plain rule's shape unless the model predicts the other one at
+        // least 10% faster (the row-bin scheduler's margin)
         float x[NFEAT], h1[MLP_H], h2[MLP_H], out[NV];
         mlp_forward(d_mlp_bc, f, x, h1, h2, out);
-        mode = out[BC_PUSH] < out[BC_PULL] ? BC_PUSH : BC_PULL;
+        const int plain = bc_plain_shape(st, m, nnz, W);
+        mode = out[plain] - out[1 - plain] >= 0.1375f ? 1 - plain : plain;
     } else {
         mode = bc_plain_shape(st, m, nnz, W);
     }

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
                         }
                         if (!skip)
                             stream_row<SUB, CAP, PKV, ACC, VAL, (FWORDS > 0 ? FLOG : 0)>(
-                                p, cur.b0, cur.b1, sl, cur.av, pkeys, acc, probe_arg, cnt, pfilt);
+                                p, cur.b0, cur.b1, sl, cur.av, pkeys, acc, probe_arg, cnt, pfilt, hi_col);
                     }
                     tc = tn;
                     tn = tnn;

@@ -4,7 +4,8 @@
 // entries with support < k-2 (keeping the others with value 1), until nnz
 // stops changing, at most n passes.  The reference compacts serially on the
 // host (:110-119); here one pass is
-//   1. support  S<C> = C·C (plus-pair) with the masked SpGEMM engine (EPI_WRITE)
+//   1. support  S<C> = C·C (plus-pair) with the masked SpGEMM engine (EPI_WRITE);
+//               for a symmetric C only its lower triangle is computed (below)
 //   2. flag     keep[j] = S[j] >= k-2
 //   3. scan     exclusive prefix of keep over all entries (one device scan)
 //   4. compact  new_rp[i] = pos[rp[i]], new_col[pos[j]] = col[j] for kept j
@@ -68,6 +69,86 @@ __global__ void k_copy_back(int64_t m, const int64_t *nrp, const int32_t *ncol, 
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += stride) col[j] = ncol[j];
 }
 
+// ---- symmetric input: support on the lower triangle only -------------------
+// For a symmetric C, S = C·C is symmetric (S_ij = |N(i) ∩ N(j)| = S_ji), so the
+// pass computes S<L> = C·C with L the strict lower triangle of C and reads the
+// support of an upper entry (i, j > i) at its mirror (j, i) in L.  The B rows
+// streamed for row i then stop at row i's largest lower column (the engine
+// ends a B row past the mask's last column), which roughly halves the streamed
+// entries.  The values are the same integers, so the truss is unchanged.
+
+// Whether every entry (i, j) has its mirror (j, i): warp per row, a binary
+// search in row j per entry.
+__global__ void k_sym_check(int64_t m, const int64_t *rp, const int32_t *col, int *asym) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
+        for (int64_t p = rp[i] + lane; p < rp[i + 1]; p += 32) {
+            const int j = col[p];
+            int64_t lo = rp[j], hi = rp[j + 1];
+            while (lo < hi) {
+                const int64_t md = (lo + hi) >> 1;
+                if (col[md] < i) lo = md + 1;
+                else hi = md;
+            }
+            if (lo == rp[j + 1] || col[lo] != i) atomicExch(asym, 1);
+        }
+    }
+}
+
+// Entries of row i below the diagonal (a prefix of the sorted row).
+__global__ void k_lower_len(int64_t m, const int64_t *rp, const int32_t *col, int64_t *len) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        int64_t lo = rp[i], hi = rp[i + 1];
+        while (lo < hi) {
+            const int64_t md = (lo + hi) >> 1;
+            if (col[md] < i) lo = md + 1;
+            else hi = md;
+        }
+        len[i] = lo - rp[i];
+    }
+}
+
+__global__ void k_lower_fill(int64_t m, const int64_t *rp, const int32_t *col, const int64_t *lrp, int32_t *lcol) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
+        const int64_t n = lrp[i + 1] - lrp[i];
+        for (int64_t k = lane; k < n; k += 32) lcol[lrp[i] + k] = col[rp[i] + k];
+    }
+}
+
+// keep[p] for every entry of C from the lower supports: a lower entry reads
+// its own position in L, an upper entry (i, j) the position of i in L's row j.
+__global__ void k_keep_sym(int64_t m, int64_t cap, const int64_t *rp, const int32_t *col, const int64_t *lrp,
+                           const int32_t *lcol, const int32_t *sup, int thresh, int32_t *keep) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
+        const int64_t e0 = rp[i], e1 = rp[i + 1];
+        for (int64_t p = e0 + lane; p < e1; p += 32) {
+            const int j = col[p];
+            int64_t q;
+            if (j < i) {
+                q = lrp[i] + (p - e0);
+            } else {
+                int64_t lo = lrp[j], hi = lrp[j + 1];
+                while (lo < hi) {
+                    const int64_t md = (lo + hi) >> 1;
+                    if (lcol[md] < i) lo = md + 1;
+                    else hi = md;
+                }
+                q = (lo < lrp[j + 1] && lcol[lo] == i) ? lo : -1;
+            }
+            keep[p] = (q >= 0 && sup[q] >= thresh) ? 1 : 0;
+        }
+    }
+    const int64_t nnz = rp[m];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = nnz + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p <= cap; p += stride) keep[p] = 0;
+}
+
 struct KtBuffers {
     int64_t m, cap;            // rows, nnz of the input (capacity of every edge array)
     int64_t *rp, *nrp;         // current / pruned row pointers
@@ -80,6 +161,9 @@ struct KtBuffers {
     size_t arena_bytes;
     KtState *st;
     int k, sched;
+    bool sym;                  // symmetric input: support on the lower triangle
+    int64_t *llen, *lrp;       // lower-triangle lengths (m + 1) and row pointers (m + 1)
+    int32_t *lcol;             // lower-triangle columns
 };
 
 // One pass: support S<C> = C·C, flags, scan, compaction, pass end, copy back.
@@ -94,9 +178,20 @@ static int ktruss_pass(const KtBuffers &b, cudaStream_t s, cudaGraphConditionalH
     rq.sched = b.sched;
     rq.c_val = b.sup;
     rq.stream = s;
-    GK_CHECK(run_spgemm(rq, pass));
-    k_keep_flags<<<sms * 8, 256, 0, s>>>(b.sup, b.rp, b.m, b.cap, b.k - 2, b.keep);
     size_t scan_bytes = b.scan_bytes;
+    if (b.sym) {
+        k_lower_len<<<sms * 4, 256, 0, s>>>(b.m, b.rp, b.col, b.llen);
+        GK_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, scan_bytes, b.llen, b.lrp, b.m + 1, s));
+        k_lower_fill<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.col, b.lrp, b.lcol);
+        rq.M = DevCsr{b.m, b.m, b.cap, b.lrp, b.lcol, nullptr};
+        GK_CHECK(run_spgemm(rq, pass));
+        k_keep_sym<<<sms * 8, 256, 0, s>>>(b.m, b.cap, b.rp, b.col, b.lrp, b.lcol, b.sup, b.k - 2, b.keep);
+        note_launches(3);
+    } else {
+        GK_CHECK(run_spgemm(rq, pass));
+        k_keep_flags<<<sms * 8, 256, 0, s>>>(b.sup, b.rp, b.m, b.cap, b.k - 2, b.keep);
+    }
+    scan_bytes = b.scan_bytes;
     GK_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, scan_bytes, b.keep, b.pos, b.cap + 1, s));
     k_compact<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.col, b.keep, b.pos, b.nrp, b.ncol);
     k_pass_end<<<1, 1, 0, s>>>(b.rp, b.nrp, b.m, static_cast<long long>(b.m), b.st, h, in_graph ? 1 : 0);
@@ -178,8 +273,28 @@ int ktruss_device(int64_t m, int64_t nnz0, int64_t *rp_a, int32_t *col_a, int k,
     GK_CHECK(scr.alloc(&b.keep, nnz0 + 1));
     GK_CHECK(scr.alloc(&b.pos, nnz0 + 1));
     GK_CHECK(scr.alloc(&b.st, 1));
+    GK_CHECK(scr.alloc(&b.llen, m + 1));
+    GK_CHECK(scr.alloc(&b.lrp, m + 1));
+    GK_CHECK(scr.alloc(&b.lcol, nnz0));
+    GK_CUDA(cudaMemsetAsync(b.llen + m, 0, sizeof(int64_t), s));
+    {
+        int *asym;
+        GK_CHECK(scr.alloc(&asym, 1));
+        GK_CUDA(cudaMemsetAsync(asym, 0, sizeof(int), s));
+        k_sym_check<<<ctx().num_sms * 8, 256, 0, s>>>(m, rp_a, col_a, asym);
+        note_launches(1);
+        int h = 1;
+        GK_CUDA(cudaMemcpyAsync(&h, asym, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GK_CUDA(cudaStreamSynchronize(s));
+        b.sym = h == 0;
+    }
     b.scan_bytes = 0;
     GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b.scan_bytes, b.keep, b.pos, nnz0 + 1, s));
+    {
+        size_t lb = 0;
+        GK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, lb, b.llen, b.lrp, m + 1, s));
+        if (lb > b.scan_bytes) b.scan_bytes = lb;
+    }
     GK_CHECK(scr.alloc(reinterpret_cast<char **>(&b.scan_tmp), b.scan_bytes));
     b.arena_bytes = spgemm_scratch_bytes(m);
     GK_CHECK(scr.alloc(reinterpret_cast<char **>(&b.arena), b.arena_bytes));

@@ -67,7 +67,12 @@ __host__ __device__ inline int forced_variant(int bin, const BinStats &b, int ac
     }
 }
 
-__device__ inline int mlp_variant(const float *w, const float *f_raw, int bin) {
+// The learned choice replaces the plain one only where the model predicts it
+// at least this much faster (log2 of 1.1): small predicted gains are within the
+// model's error and are not worth a change of kernel.
+constexpr float LEARNED_MARGIN = 0.1375f;
+
+__device__ inline int mlp_variant(const float *w, const float *f_raw, int bin, int plain) {
     const float *W1 = w;
     const float *b1 = W1 + MLP_H * NFEAT;
     const float *W2 = b1 + MLP_H;
@@ -89,17 +94,18 @@ __device__ inline int mlp_variant(const float *w, const float *f_raw, int bin) {
         h2[j] = a > 0.f ? a : 0.f;
     }
     int best = 6;  // allowed for every bin
-    float best_s = 3.0e38f;
+    float best_s = 3.0e38f, plain_s = 3.0e38f;
     for (int v = 0; v < NV; ++v) {
-        if (!variant_allowed(v, bin)) continue;
+        if (!variant_allowed(v, bin) && v != plain) continue;
         float a = b3[v];
         for (int i = 0; i < MLP_H; ++i) a += W3[v * MLP_H + i] * h2[i];
-        if (a < best_s) {
+        if (v == plain) plain_s = a;
+        if (variant_allowed(v, bin) && a < best_s) {
             best_s = a;
             best = v;
         }
     }
-    return best;
+    return plain_s - best_s >= LEARNED_MARGIN ? best : plain;
 }
 
 __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int accum, int epi, bool values) {
@@ -115,7 +121,7 @@ __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int ac
     else if (mode == GK_SCHED_LEARNED) {
         float f[NFEAT];
         bin_features(st, epi, values, f);
-        v = mlp_variant(d_mlp, f, b);
+        v = mlp_variant(d_mlp, f, b, plain_variant(b, st));
     } else v = plain_variant(b, st);
     var_of_bin[b] = v;
 }

@@ -288,11 +288,13 @@ __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int
 // The SUB lanes of a sub-group stream B[b0, b1): 16-byte vector loads, two in
 // flight per lane, scalar head/tail; with values, scalar loads of col and val.
 // With a filter, the eight elements of two vectors are tested against the
-// filter without branches and only the candidates take the exact lookup.
+// filter without branches and only the candidates take the exact lookup.  A
+// lane stops once its elements pass hi_col, the last mask column of the
+// item (B rows are sorted); elements beyond it could never match.
 template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0>
 __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b1, int sl, uint32_t av,
                                            const int *keys, int *acc, int clen, unsigned &cnt,
-                                           const unsigned *filt = nullptr) {
+                                           const unsigned *filt, int hi_col) {
     const int32_t *__restrict__ bc = p.B.col;
     if constexpr (PK == PK_HASH && FLOG > 0 && !VAL) {
         if (p.vec) {
@@ -302,6 +304,7 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             const int4 *__restrict__ base = reinterpret_cast<const int4 *>(bc) + (h1 >> 2);
             const int n4 = static_cast<int>((b1 >> 2) - (h1 >> 2));
             int q = sl;
+            bool past = false;  // this lane's elements went beyond the mask's last column
             for (; q + SUB < n4; q += 2 * SUB) {
                 const int4 x = __ldg(base + q);
                 const int4 y = __ldg(base + q + SUB);
@@ -310,8 +313,12 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
                                    (cand_bit<FLOG>(y.x, filt) << 4) | (cand_bit<FLOG>(y.y, filt) << 5) |
                                    (cand_bit<FLOG>(y.z, filt) << 6) | (cand_bit<FLOG>(y.w, filt) << 7);
                 exact_cands<CAP, ACC>(m, x, y, av, keys, acc, cnt);
+                if (y.w > hi_col) {  // B rows are sorted: the rest cannot be mask columns
+                    past = true;
+                    break;
+                }
             }
-            if (q < n4) {
+            if (!past && q < n4) {
                 const int4 x = __ldg(base + q);
                 const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
                                    (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3);
@@ -330,6 +337,7 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
         const int64_t v1 = b1 >> 2;
         const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
         int64_t q = (h1 >> 2) + sl;
+        bool past = false;
         for (; q + SUB < v1; q += 2 * SUB) {
             const int4 x = __ldg(bv + q);
             const int4 y = __ldg(bv + q + SUB);
@@ -341,8 +349,12 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             probe_elem<CAP, PK, ACC, FLOG>(y.y, av, keys, acc, clen, cnt, filt);
             probe_elem<CAP, PK, ACC, FLOG>(y.z, av, keys, acc, clen, cnt, filt);
             probe_elem<CAP, PK, ACC, FLOG>(y.w, av, keys, acc, clen, cnt, filt);
+            if (y.w > hi_col) {
+                past = true;
+                break;
+            }
         }
-        if (q < v1) {
+        if (!past && q < v1) {
             const int4 x = __ldg(bv + q);
             probe_elem<CAP, PK, ACC, FLOG>(x.x, av, keys, acc, clen, cnt, filt);
             probe_elem<CAP, PK, ACC, FLOG>(x.y, av, keys, acc, clen, cnt, filt);
@@ -355,8 +367,10 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
     } else {
         const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
         for (int64_t j = b0 + sl; j < b1; j += SUB) {
+            const int x = __ldg(bc + j);
+            if (x > hi_col) break;
             const uint32_t w = (VAL && bvals) ? av * static_cast<uint32_t>(__ldg(bvals + j)) : av;
-            probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + j), w, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG>(x, w, keys, acc, clen, cnt, filt);
         }
     }
 }
@@ -404,11 +418,17 @@ __device__ __forceinline__ void stream_entries(const KArgs &p, int64_t first, in
                 }
             }
             if (!skip)
-                stream_row<SUB, CAP, PK, ACC, VAL, FLOG>(p, cur.b0, cur.b1, sl, cur.av, keys, acc, clen, cnt, filt);
+                stream_row<SUB, CAP, PK, ACC, VAL, FLOG>(p, cur.b0, cur.b1, sl, cur.av, keys, acc, clen, cnt, filt,
+                                                         hi_col);
         }
         t = tn;
     }
 }
+
+// Rows a group takes per fetch: four for the narrow groups, whose rows are
+// short, so that the shared counter is not hit once per row.
+template <int G>
+__host__ __device__ constexpr int c_group_fetch() { return G >= 32 ? 2 : 4; }
 
 // G threads per row; the row's A entries are dealt round-robin to G/SUB
 // sub-groups of SUB lanes that stream their B rows concurrently.  Each group
@@ -430,11 +450,30 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
     const unsigned gmask = group_mask<G>();
     const int begin = p.voff[p.v], end = p.voff[p.v + 1];
     unsigned long long local = 0;
+    // keyed sums: consecutive rows of a group mostly share a key (rows of one
+    // graph of a batch), so a group adds up per key and flushes on change
+    int cur_key = -1;
+    unsigned long long cur_sum = 0;
+    // the table and filter start empty; every row clears what it set
+    if constexpr (!MCA) {
+        for (int s = lane; s < CAP; s += G) {
+            keys[s] = EMPTY_KEY;
+            if (ACC) acc[s] = 0;
+        }
+        for (int wd = lane; wd < FW; wd += G) filt[wd] = 0u;
+    }
+    __syncwarp(gmask);
+    constexpr int FB = c_group_fetch<G>();
+    int got = 0, left = 0;
 
     while (true) {
-        int got = 0;
-        if (lane == 0) got = static_cast<int>(atomicAdd(p.fetch + p.v, 1u));
-        const int idx = begin + __shfl_sync(gmask, got, 0, G);
+        if (left == 0) {
+            if (lane == 0) got = static_cast<int>(atomicAdd(p.fetch + p.v, static_cast<unsigned>(FB)));
+            got = __shfl_sync(gmask, got, 0, G);
+            left = FB;
+        }
+        const int idx = begin + got + (FB - left);
+        --left;
         if (idx >= end) break;
         const int row = p.rowlist[idx];
         const int64_t m0 = p.M.rp[row];
@@ -452,12 +491,6 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
                     if (ACC) acc[q] = 0;
                 }
             } else {
-                for (int s = lane; s < CAP; s += G) {
-                    keys[s] = EMPTY_KEY;
-                    if (ACC) acc[s] = 0;
-                }
-                for (int wd = lane; wd < FW; wd += G) filt[wd] = 0u;
-                __syncwarp(gmask);
                 for (int q = c0 + lane; q < c1; q += G) {
                     const int x = mc[q];
                     hash_insert<CAP>(keys, x);
@@ -472,22 +505,53 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
             unsigned cnt = 0;
             stream_entries<SUB, CAP, MCA ? PK_MCA : PK_HASH, ACC, VAL, (FW > 0 ? FLOG : 0)>(
                 p, a0 + sg, a1, S, sl, chunked, lo_col, hi_col, keys, acc, clen, cnt, filt);
-            if (ACC) {
-                __syncwarp(gmask);
-                for (int q = c0 + lane; q < c1; q += G) {
-                    const int s = MCA ? (q - c0) : hash_find<CAP>(keys, mc[q]);
-                    p.c_val[m0 + q] = acc[s];
-                }
+            __syncwarp(gmask);
+            if constexpr (MCA) {
+                if (ACC)
+                    for (int q = c0 + lane; q < c1; q += G) p.c_val[m0 + q] = acc[q - c0];
             } else {
-                rowsum += cnt;
+                // find this chunk's slots (writing the values out), then clear
+                // them and the filter words only after every lane has found
+                // its keys, so that no probe meets a half-cleared bucket
+                constexpr int PER = (CHUNK + G - 1) / G;
+                int slot[PER];
+#pragma unroll
+                for (int k = 0; k < PER; ++k) {
+                    const int q = c0 + lane + k * G;
+                    slot[k] = q < c1 ? hash_find<CAP>(keys, mc[q]) : -1;
+                    if (ACC && slot[k] >= 0) p.c_val[m0 + q] = acc[slot[k]];
+                }
+                __syncwarp(gmask);
+#pragma unroll
+                for (int k = 0; k < PER; ++k) {
+                    const int q = c0 + lane + k * G;
+                    if (slot[k] >= 0) {
+                        keys[slot[k]] = EMPTY_KEY;
+                        if (ACC) acc[slot[k]] = 0;
+                    }
+                    if constexpr (FW > 0) {
+                        if (q < c1) filt[filter_bit<FLOG>(mc[q]) >> 5] = 0u;
+                    }
+                }
             }
+            if (!ACC) rowsum += cnt;
             __syncwarp(gmask);
         }
         if (EPI == EPI_SUM) local += rowsum;
         if (EPI == EPI_KEYED) {
-            const unsigned long long tot = group_sum<G>(rowsum, gmask);
-            if (lane == 0 && tot) atomicAdd(p.sums + (p.row_key ? p.row_key[row] : row), tot);
+            const int key = p.row_key ? p.row_key[row] : row;
+            if (key != cur_key) {
+                const unsigned long long tot = group_sum<G>(cur_sum, gmask);
+                if (lane == 0 && tot) atomicAdd(p.sums + cur_key, tot);
+                cur_key = key;
+                cur_sum = 0;
+            }
+            cur_sum += rowsum;
         }
+    }
+    if (EPI == EPI_KEYED && cur_key >= 0) {
+        const unsigned long long tot = group_sum<G>(cur_sum, gmask);
+        if (lane == 0 && tot) atomicAdd(p.sums + cur_key, tot);
     }
     if (EPI == EPI_SUM) {
         // groups leave at different times: reduce per group, no CTA barrier

@@ -13,8 +13,11 @@ namespace gk {
 void bin_features_host(const BinStats &b, int epi, bool values, float *f);
 int plain_variant_host(int bin, const BinStats &b);
 
+int extract_lower_device(const DevCsr &A, int64_t *orp, int32_t *ocol, cudaStream_t s, Scratch &scr);
+
 // mode 0: triangle counting on L (A = B = M = L, sum of C);
-// mode 1: k-truss support on a symmetric A (A = B = M, values written).
+// mode 1: k-truss support on a symmetric A as gk_ktruss computes it
+//         (A = B = the symmetric matrix, M = its strict lower triangle, values written).
 static int tune_request(const gk_csr *G, int mode, SpgemmRequest &rq, Scratch &scr, cudaStream_t s,
                         unsigned long long **sums, int32_t **cval) {
     if (mode != 0 && mode != 1) return fail(GK_ERR_ARG, "tune: mode must be 0 (triangle count) or 1 (k-truss support)");
@@ -34,6 +37,12 @@ static int tune_request(const gk_csr *G, int mode, SpgemmRequest &rq, Scratch &s
         GK_CHECK(scr.alloc(cval, d.nnz > 0 ? d.nnz : 1));
         rq.epi = EPI_WRITE;
         rq.c_val = *cval;
+        int64_t *lrp;
+        int32_t *lcol;
+        GK_CHECK(scr.alloc(&lrp, d.m + 1));
+        GK_CHECK(scr.alloc(&lcol, d.nnz > 0 ? d.nnz : 1));
+        GK_CHECK(extract_lower_device(d, lrp, lcol, s, scr));
+        rq.M = DevCsr{d.m, d.n, d.nnz, lrp, lcol, nullptr};
     }
     return GK_OK;
 }

@@ -208,6 +208,19 @@ def train(X, Y, M, epochs=4000, lr=3e-3, seed=0):
     return w, trace
 
 
+def train_best(X, Y, M, recs, epochs, seeds, evaluate_fn):
+    """Trains from `seeds` initialisations and keeps the network whose choices
+    take the least measured time on the sweep (the MLP's argmin is sensitive to
+    small prediction errors between close variants)."""
+    best = None
+    for seed in range(seeds):
+        w, trace = train(X, Y, M, epochs=epochs, seed=seed)
+        ev = evaluate_fn(w)
+        if best is None or ev["learned_ms"] < best[2]["learned_ms"]:
+            best = (w, trace, ev)
+    return best
+
+
 def forward_gpu(w, X):
     lib = _lib.load()
     nv, nf, nb = dims()
@@ -236,12 +249,19 @@ def forward_numpy(w, X, nf, nv):
     return h2 @ W3.T + b3
 
 
+LEARNED_MARGIN = 0.1375  # log2(1.1): the model must predict >= 10% gain over the plain pick
+
+
 def choose(out, recs):
-    """argmin over each bin's admissible variants (as the device inference does)."""
+    """As the device inference does: argmin over the bin's admissible
+    variants, kept only where it is predicted LEARNED_MARGIN (log2) faster
+    than the plain heuristic's variant."""
     picks = []
     for i, r in enumerate(recs):
         cand = [v for v in range(out.shape[1]) if allowed(r["bin"], v)]
-        picks.append(min(cand, key=lambda v: out[i, v]))
+        best = min(cand, key=lambda v: out[i, v])
+        p = r["plain"]
+        picks.append(best if out[i, p] - out[i, best] >= LEARNED_MARGIN else p)
     return picks
 
 
@@ -341,8 +361,14 @@ def bc_dataset(recs):
     return X, Y, M
 
 
-def bc_choose(out):
-    return [BC_PUSH if o[BC_PUSH] < o[BC_PULL] else BC_PULL for o in out]
+def bc_choose(out, recs):
+    """The plain rule's shape unless the model predicts the other one
+    LEARNED_MARGIN (log2) faster (as k_bc_choose does)."""
+    picks = []
+    for o, r in zip(out, recs):
+        p = r["plain"]
+        picks.append(1 - p if o[p] - o[1 - p] >= LEARNED_MARGIN else p)
+    return picks
 
 
 def bc_evaluate(recs, picks):
@@ -379,6 +405,7 @@ TRAIN_GRAPHS = [
     ("er1m-d16-s16", dict(kind="er", n=1 << 20, nedges=8 << 20, seed=16)),
     ("er4m-d32-s17", dict(kind="er", n=1 << 22, nedges=64 << 20, seed=17)),
     ("batch512-s5000", dict(kind="batch", ngraphs=512, seed0=5000)),
+    ("batch1024-s7000", dict(kind="batch", ngraphs=1024, seed0=7000)),
 ]
 KTRUSS_GRAPHS = [
     ("rmat18-s18", dict(kind="rmat", scale=18, seed=18)),
@@ -411,6 +438,7 @@ def main():
     ap.add_argument("--train", action="store_true", help="sweep the training graphs, train and save the model")
     ap.add_argument("--retrain", action="store_true", help="train from the saved sweep without re-measuring")
     ap.add_argument("--epochs", type=int, default=4000)
+    ap.add_argument("--seeds", type=int, default=6, help="initialisations to train; the best on the sweep is kept")
     ap.add_argument("--max-scale", type=int, default=24)
     ap.add_argument("--out", default=MODEL_DIR, help="directory for model.npz (and sweep.npz with --train)")
     ap.add_argument("--data", default=DATA_PATH, help="sweep to train from with --retrain")
@@ -443,9 +471,8 @@ def main():
         save_dataset(recs, data_path)
     recs = load_dataset(data_path)
     X, Y, M = to_dataset(recs)
-    w, trace = train(X, Y, M, epochs=args.epochs)
-    picks = choose(forward_gpu(w, X), recs)
-    ev = evaluate(recs, picks)
+    w, trace, ev = train_best(X, Y, M, recs, args.epochs, args.seeds,
+                              lambda w_: evaluate(recs, choose(forward_gpu(w_, X), recs)))
     print(json.dumps({"samples": len(recs), "loss_first": float(trace[0]), "loss_last": float(trace[-1]), **ev}))
     save_model(w, model_path, samples=len(recs), epochs=args.epochs, final_loss=float(trace[-1]), **ev)
 
@@ -465,9 +492,8 @@ def main_bc(args):
         save_dataset(recs, data_path)
     recs = load_bc_dataset(data_path)
     X, Y, M = bc_dataset(recs)
-    w, trace = train(X, Y, M, epochs=args.epochs)
-    picks = bc_choose(forward_gpu(w, X))
-    ev = bc_evaluate(recs, picks)
+    w, trace, ev = train_best(X, Y, M, recs, args.epochs, args.seeds,
+                              lambda w_: bc_evaluate(recs, bc_choose(forward_gpu(w_, X), recs)))
     print(json.dumps({"samples": len(recs), "loss_first": float(trace[0]), "loss_last": float(trace[-1]), **ev}))
     save_model(w, model_path, samples=len(recs), epochs=args.epochs, final_loss=float(trace[-1]), **ev)
 

@@ -62,6 +62,27 @@ def test_ktruss_fixed_point(gk, cuda):
     assert it2 == 1 and T2.nnz == T.nnz
 
 
+def test_ktruss_nonsymmetric_input(gk, orc, cuda):
+    """A non-symmetric matrix takes the full-mask support S<C> = C·C (the
+    lower-triangle shortcut needs S = S^T) and still matches the oracle."""
+    for seed in (5, 6):
+        A = G.random_csr(400, 400, 0.06, seed=seed)
+        # no self-loops, as the k-truss input requires
+        rp, col = np.asarray(A.rowptr), np.asarray(A.col)
+        rows = np.repeat(np.arange(A.m), np.diff(rp))
+        keep = col != rows
+        B = G.from_pairs(A.m, rows[keep], col[keep]) if hasattr(G, "from_pairs") else None
+        if B is None:
+            nrp = np.zeros(A.m + 1, dtype=np.int64)
+            np.cumsum(np.bincount(rows[keep], minlength=A.m), out=nrp[1:])
+            B = gk.Csr(A.m, A.m, nrp, col[keep].astype(np.int32), None, int(keep.sum()))
+        want_rp, want_col, want_it, _ = orc.ktruss(B, 3)
+        T, it = gk.ktruss(dev(B), 3)
+        assert it == want_it and T.nnz == len(want_col)
+        np.testing.assert_array_equal(T.rowptr.cpu().numpy(), want_rp)
+        np.testing.assert_array_equal(T.col.cpu().numpy(), want_col)
+
+
 def test_ktruss_graph_loop_matches_host_loop(gk, cuda):
     """The pass loop runs as one CUDA graph (conditional while node); with
     profiling on the host drives the same passes.  Both, and both schedulers,
