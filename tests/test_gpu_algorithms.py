@@ -71,11 +71,9 @@ def test_ktruss_nonsymmetric_input(gk, orc, cuda):
         rp, col = np.asarray(A.rowptr), np.asarray(A.col)
         rows = np.repeat(np.arange(A.m), np.diff(rp))
         keep = col != rows
-        B = G.from_pairs(A.m, rows[keep], col[keep]) if hasattr(G, "from_pairs") else None
-        if B is None:
-            nrp = np.zeros(A.m + 1, dtype=np.int64)
-            np.cumsum(np.bincount(rows[keep], minlength=A.m), out=nrp[1:])
-            B = gk.Csr(A.m, A.m, nrp, col[keep].astype(np.int32), None, int(keep.sum()))
+        nrp = np.zeros(A.m + 1, dtype=np.int64)
+        np.cumsum(np.bincount(rows[keep], minlength=A.m), out=nrp[1:])
+        B = gk.Csr(A.m, A.m, nrp, col[keep].astype(np.int32), None, int(keep.sum()))
         want_rp, want_col, want_it, _ = orc.ktruss(B, 3)
         T, it = gk.ktruss(dev(B), 3)
         assert it == want_it and T.nnz == len(want_col)
