@@ -216,8 +216,17 @@ __device__ int bc_plain_shape(const BcState *st, int64_t m, int64_t nnz, int W) 
 
 // Picks the forward shape of level st->d (force >= 0 overrides) and logs the
 // level's features when feat_log is given.
+// One warp: the lanes stage the model's weights in shared memory, lane 0
+// decides.
 __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_t nnz, int W, float *feat_log,
                             int log_cap) {
+    __shared__ float sw[MLP_SIZE];
+    const bool learned = force < 0 && sched == GK_SCHED_LEARNED;
+    if (learned) {
+        for (int i = threadIdx.x; i < MLP_SIZE; i += blockDim.x) sw[i] = d_mlp_bc[i];
+        __syncwarp();
+    }
+    if (threadIdx.x != 0) return;
     float f[BC_FEAT];
     bc_features(st, m, nnz, W, f);
     int mode;
@@ -227,7 +236,7 @@ __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_
         // the plain rule's shape unless the model predicts the other one at
         // least 10% faster (the row-bin scheduler's margin)
         float x[NFEAT], h1[MLP_H], h2[MLP_H], out[NV];
-        mlp_forward(d_mlp_bc, f, x, h1, h2, out);
+        mlp_forward(sw, f, x, h1, h2, out);
         const int plain = bc_plain_shape(st, m, nnz, W);
         mode = out[plain] - out[1 - plain] >= 0.1375f ? 1 - plain : plain;
     } else {
@@ -903,7 +912,7 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
 
         // ---- forward levels ----
         auto fwd_level = [&](cudaStream_t ls, cudaGraphConditionalHandle h, bool in_graph) {
-            k_bc_choose<<<1, 1, 0, ls>>>(st, opt.force, opt.sched, m, nnz, W, feat_dev, opt.log_cap);
+            k_bc_choose<<<1, 32, 0, ls>>>(st, opt.force, opt.sched, m, nnz, W, feat_dev, opt.log_cap);
             k_bc_pull<T><<<sms * 8, 256, 0, ls>>>(g.AT, g.A, st, V, sigma, W, act);
             int k = 0;
             if (g.hAT.n) {

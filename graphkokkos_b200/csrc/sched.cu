@@ -109,6 +109,14 @@ __device__ inline int mlp_variant(const float *w, const float *f_raw, int bin, i
 }
 
 __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int accum, int epi, bool values) {
+    // the weights are read by every bin's thread: stage them in shared memory
+    // (broadcast reads) instead of chains of dependent global loads
+    __shared__ float sw[MLP_SIZE];
+    const bool learned = mode == GK_SCHED_LEARNED && accum == GK_ACCUM_AUTO;
+    if (learned) {
+        for (int i = threadIdx.x; i < MLP_SIZE; i += blockDim.x) sw[i] = d_mlp[i];
+        __syncthreads();
+    }
     const int b = threadIdx.x + blockIdx.x * blockDim.x;
     if (b >= NBINS) return;
     const BinStats st = bins[b];
@@ -121,7 +129,7 @@ __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int ac
     else if (mode == GK_SCHED_LEARNED) {
         float f[NFEAT];
         bin_features(st, epi, values, f);
-        v = mlp_variant(d_mlp, f, b, plain_variant(b, st));
+        v = mlp_variant(sw, f, b, plain_variant(b, st));
     } else v = plain_variant(b, st);
     var_of_bin[b] = v;
 }
