@@ -172,6 +172,26 @@ def tc_row_sums(L: Csr, sched="plain", stream=None):
     return out
 
 
+def tc_vertex(A: Csr, sched="plain", stream=None):
+    """Triangles through each vertex of a symmetric adjacency
+    (triangle_counting_vertex, src/main.cpp:16-39); int32 per vertex."""
+    lib = _lib.load()
+    out = _empty_like_space(A.rowptr, (A.m,), np.int32)
+    g = A.as_gk()
+    check(lib.gk_tc_vertex(ctypes.byref(g), _ptr(out), _SCHED[sched], _stream(stream, A.col)))
+    return out
+
+
+def tc_count_lu(A: Csr, sched="plain", stream=None) -> int:
+    """Triangle count as sum(C<A> = L·U) / 2 (triangle_counting_masked_lu,
+    src/main.cpp:42-66), from the symmetric adjacency A."""
+    lib = _lib.load()
+    out = ctypes.c_uint64(0)
+    g = A.as_gk()
+    check(lib.gk_tc_count_lu(ctypes.byref(g), ctypes.addressof(out), _SCHED[sched], _stream(stream, A.col)))
+    return int(out.value)
+
+
 def tc_count_batched(graphs: Sequence[Csr], sched="plain", stream=None):
     lib = _lib.load()
     n = len(graphs)

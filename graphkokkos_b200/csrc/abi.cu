@@ -24,6 +24,14 @@ static int deliver(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     return GK_OK;
 }
 
+// (sum >> 1) as the reference's int per vertex (src/main.cpp:27-31)
+__global__ void k_half_int(int64_t m, const unsigned long long *sums, int32_t *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = static_cast<int32_t>(static_cast<int64_t>(sums[i]) >> 1);
+}
+
+__global__ void k_half_u64(const unsigned long long *sum, unsigned long long *half) { *half = *sum >> 1; }
+
 static int check_square_pattern(const gk_csr *L, const char *name) {
     GK_CHECK(validate_csr_shape(L, name));
     if (L->m != L->n) return fail(GK_ERR_ARG, std::string(name) + ": matrix must be square");
@@ -281,6 +289,73 @@ int gk_tc_row_sums(const gk_csr *L, uint64_t *row_sums, int sched, void *stream)
     GK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * (L->m + 1), s));
     GK_CHECK(tc_common(L, EPI_KEYED, d, sched, s, scr));
     return deliver(row_sums, d, sizeof(uint64_t) * L->m, s);
+}
+
+int gk_tc_vertex(const gk_csr *A, int32_t *counts, int sched, void *stream) {
+    GK_CHECK(check_square_pattern(A, "A"));
+    if (!counts && A->m > 0) return fail(GK_ERR_ARG, "counts is null");
+    if (A->m == 0) return GK_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scr(s);
+    DevCsr d;
+    GK_CHECK(stage_csr(A, &d, scr, s));
+    d.val = nullptr;
+    unsigned long long *sums;
+    int32_t *out;
+    GK_CHECK(scr.alloc(&sums, A->m + 1));
+    GK_CHECK(scr.alloc(&out, A->m));
+    GK_CUDA(cudaMemsetAsync(sums, 0, sizeof(unsigned long long) * (A->m + 1), s));
+    SpgemmRequest rq;
+    rq.A = rq.B = rq.M = d;
+    rq.epi = EPI_KEYED;  // row sums of C<A> = A·A
+    rq.sched = sched;
+    rq.sums = sums;
+    rq.stream = s;
+    GK_CHECK(run_spgemm(rq, scr));
+    k_half_int<<<ceil_div(A->m, 256), 256, 0, s>>>(A->m, sums, out);
+    note_launches(1);
+    GK_CUDA(cudaGetLastError());
+    return deliver(counts, out, sizeof(int32_t) * A->m, s);
+}
+
+int gk_tc_count_lu(const gk_csr *A, uint64_t *count, int sched, void *stream) {
+    GK_CHECK(check_square_pattern(A, "A"));
+    if (!count) return fail(GK_ERR_ARG, "count is null");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scr(s);
+    DevCsr d;
+    GK_CHECK(stage_csr(A, &d, scr, s));
+    d.val = nullptr;
+    const int64_t m = A->m;
+    int64_t *lrp, *urp;
+    int32_t *lcol, *ucol;
+    GK_CHECK(scr.alloc(&lrp, m + 1));
+    GK_CHECK(scr.alloc(&lcol, d.nnz > 0 ? d.nnz : 1));
+    GK_CHECK(extract_lower_device(d, lrp, lcol, s, scr));
+    int64_t lnnz = 0;
+    GK_CUDA(cudaMemcpyAsync(&lnnz, lrp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    GK_CUDA(cudaStreamSynchronize(s));
+    DevCsr L{m, m, lnnz, lrp, lcol, nullptr};
+    GK_CHECK(scr.alloc(&urp, m + 1));
+    GK_CHECK(scr.alloc(&ucol, lnnz > 0 ? lnnz : 1));
+    GK_CHECK(transpose_device(L, urp, ucol, nullptr, s, scr));
+    unsigned long long *sum, *half;
+    GK_CHECK(scr.alloc(&sum, 2));
+    half = sum + 1;
+    GK_CUDA(cudaMemsetAsync(sum, 0, 2 * sizeof(unsigned long long), s));
+    SpgemmRequest rq;
+    rq.A = L;
+    rq.B = DevCsr{m, m, lnnz, urp, ucol, nullptr};
+    rq.M = d;
+    rq.epi = EPI_SUM;
+    rq.sched = sched;
+    rq.sums = sum;
+    rq.stream = s;
+    GK_CHECK(run_spgemm(rq, scr));
+    k_half_u64<<<1, 1, 0, s>>>(sum, half);
+    note_launches(1);
+    GK_CUDA(cudaGetLastError());
+    return deliver(count, half, sizeof(uint64_t), s);
 }
 
 int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int sched, void *stream) {

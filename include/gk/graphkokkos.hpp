@@ -11,6 +11,8 @@
 //                       include/matrix_la.h:478-694, :936-1068 — C<M> = A·B, C
 //                       resized to M's pattern with explicit zeros kept (:564-568)
 //   triangle_counting_masked_sandia   src/main.cpp:69-90
+//   triangle_counting_vertex          src/main.cpp:16-39
+//   triangle_counting_masked_lu       src/main.cpp:42-66
 //   k_truss                           src/main.cpp:94-141
 //   betweenness_centrality_batch      include/betweenness_centrality.h:406-506
 //   transpose / extract_lower_triangle / build_symm_from_lower /
@@ -260,6 +262,56 @@ inline int64_t triangle_counting_masked_sandia(const spMtx<int> &A, mxmOp<int> m
     int64_t sum = 0;
     for (size_t j = 0; j < C.nz; ++j) sum += C.Val(j);
     return sum;
+}
+
+// Triangles through each vertex (src/main.cpp:16-39): a new[]'d array of A.m
+// ints the caller deletes, as in the reference.  With one of this header's
+// operators the row sums of C<A> = A·A are fused on the GPU.
+inline int *triangle_counting_vertex(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel) {
+    int *nums = new int[A.m];
+    const bool ours = matrixMult == static_cast<mxmOp<int>>(mxmm_msa<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_mca<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_naive<int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_gpu<int>);
+    if (ours) {
+        gk_csr a = A.csr(false);
+        try {
+            gkb_detail::check(gk_tc_vertex(&a, reinterpret_cast<int32_t *>(nums), GK_SCHED_PLAIN, nullptr));
+        } catch (...) {
+            delete[] nums;
+            throw;
+        }
+        return nums;
+    }
+    spMtx<int> SQ;
+    matrixMult(isParallel, A, A, A, SQ);
+    for (size_t i = 0; i < A.m; ++i) {
+        int num_of_tr = 0;
+        for (int64_t j = SQ.Rst(i); j < SQ.Rst(i + 1); ++j) num_of_tr += SQ.Val(j);
+        nums[i] = num_of_tr >> 1;
+    }
+    return nums;
+}
+
+// Triangle count through C<A> = L·U, U = transpose(L) (src/main.cpp:42-66).
+inline int64_t triangle_counting_masked_lu(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel) {
+    const bool ours = matrixMult == static_cast<mxmOp<int>>(mxmm_msa<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_mca<int, int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_naive<int>) ||
+                      matrixMult == static_cast<mxmOp<int>>(mxmm_gpu<int>);
+    if (ours) {
+        gk_csr a = A.csr(false);
+        uint64_t count = 0;
+        gkb_detail::check(gk_tc_count_lu(&a, &count, GK_SCHED_PLAIN, nullptr));
+        return static_cast<int64_t>(count);
+    }
+    spMtx<int> L = extract_lower_triangle(A);
+    spMtx<int> U = transpose(L);
+    spMtx<int> C;
+    matrixMult(isParallel, L, U, A, C);
+    int64_t sum = 0;
+    for (size_t j = 0; j < C.nz; ++j) sum += C.Val(j);
+    return sum >> 1;
 }
 
 // k-truss (src/main.cpp:94-141).  matrixMult is accepted for signature

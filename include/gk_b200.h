@@ -118,6 +118,16 @@ int gk_tc_count_noalloc(const gk_csr *L, uint64_t *count, int sched, void *strea
  * triangle_counting_vertex, src/main.cpp:16-39). */
 int gk_tc_row_sums(const gk_csr *L, uint64_t *row_sums, int sched, void *stream);
 
+/* Triangles through each vertex of a symmetric adjacency A:
+ * counts[i] = (sum_j C(i,j)) >> 1 with C<A> = A·A, as int like the reference's
+ * triangle_counting_vertex (src/main.cpp:16-39).  counts has A.m entries. */
+int gk_tc_vertex(const gk_csr *A, int32_t *counts, int sched, void *stream);
+
+/* Triangle count through the L·U formulation: L = tril(A), U = L^T,
+ * *count = sum(C<A> = L·U) >> 1 (triangle_counting_masked_lu,
+ * src/main.cpp:42-66).  A: symmetric adjacency, sorted rows. */
+int gk_tc_count_lu(const gk_csr *A, uint64_t *count, int sched, void *stream);
+
 /* Triangle counts of many independent graphs in one persistent launch:
  * counts[g] = gk_tc_count(&graphs[g]).  No reference counterpart (the
  * reference runs one graph per process, src/main.cpp:323-345). */

@@ -112,6 +112,14 @@ def tc_merge(L):
     return int(out.value)
 
 
+def tc_vertex(A):
+    """Triangles through each vertex of a symmetric adjacency (int32)."""
+    m, _, rp, col, _ = _host(A)
+    out = np.zeros(m, dtype=np.int32)
+    port().orc_tc_vertex(I64(m), _p(rp), _p(col), _p(out))
+    return out
+
+
 def tc_row_sums(L):
     m, _, rp, col, _ = _host(L)
     out = np.zeros(m, dtype=np.uint64)
@@ -227,6 +235,28 @@ def ref_ktruss(A_sym, k, accum="msa", parallel=True):
     if r != 0:
         raise RuntimeError(f"reference ktruss failed ({r})")
     return orp, ocol[: nnz.value].copy(), int(iters.value)
+
+
+def ref_tc_vertex(A, accum=0, parallel=True):
+    """The reference's triangle_counting_vertex (src/main.cpp:16-39), restated
+    around its mxmm_msa / mxmm_mca."""
+    m, _, rp, col, _ = _host(A)
+    out = np.zeros(m, dtype=np.int32)
+    r = ref().ref_tc_vertex(ctypes.c_int(accum), ctypes.c_int(1 if parallel else 0), I64(m), _p(rp), _p(col), _p(out))
+    if r != 0:
+        raise RuntimeError(f"reference tc_vertex failed ({r})")
+    return out
+
+
+def ref_tc_lu(A, accum=0, parallel=True):
+    """The reference's triangle_counting_masked_lu (src/main.cpp:42-66)."""
+    m, _, rp, col, _ = _host(A)
+    out = ctypes.c_int64(0)
+    r = ref().ref_tc_lu(ctypes.c_int(accum), ctypes.c_int(1 if parallel else 0), I64(m), _p(rp), _p(col),
+                        ctypes.byref(out))
+    if r != 0:
+        raise RuntimeError(f"reference tc_lu failed ({r})")
+    return int(out.value)
 
 
 def ref_bc_float(A_sym, b, threads=1):

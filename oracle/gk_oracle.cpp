@@ -203,6 +203,27 @@ int orc_tc_row_sums(int64_t m, const int64_t *rp, const int32_t *col, uint64_t *
     return 0;
 }
 
+// triangle_counting_vertex (src/main.cpp:16-39): C<A> = A·A on the symmetric
+// adjacency A, nums[i] = (sum_j C(i,j)) >> 1, the triangles through vertex i.
+int orc_tc_vertex(int64_t m, const int64_t *rp, const int32_t *col, int32_t *out) {
+#pragma omp parallel
+    {
+        std::vector<uint8_t> mark(static_cast<size_t>(m), 0);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < m; ++i) {
+            for (int64_t j = rp[i]; j < rp[i + 1]; ++j) mark[col[j]] = 1;
+            int64_t c = 0;  // sum over the mask entries j of |A_i ∩ A_j|
+            for (int64_t t = rp[i]; t < rp[i + 1]; ++t) {
+                const int32_t k = col[t];
+                for (int64_t j = rp[k]; j < rp[k + 1]; ++j) c += mark[col[j]];
+            }
+            out[i] = static_cast<int32_t>(c >> 1);
+            for (int64_t j = rp[i]; j < rp[i + 1]; ++j) mark[col[j]] = 0;
+        }
+    }
+    return 0;
+}
+
 // Independent second method: sorted-merge intersection, sum over (i,k) in L
 // of |L_i ∩ L_k| (each triangle i>k>j counted once).
 int orc_tc_merge(int64_t m, const int64_t *rp, const int32_t *col, uint64_t *out) {

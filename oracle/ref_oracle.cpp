@@ -70,6 +70,30 @@ int64_t tc_sandia(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel) {
     return num_of_tr;
 }
 
+// Restatement of triangle_counting_vertex (src/main.cpp:16-39) without the
+// timing line: SQ<A> = A·A, nums[i] = (row sum of SQ) >> 1.
+void tc_vertex(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel, int32_t *nums) {
+    spMtx<int> SQ;
+    matrixMult(isParallel, A, A, A, SQ);
+    for (size_t i = 0; i < A.m; ++i) {
+        int num_of_tr = 0;
+        for (int j = SQ.Rst(i); j < SQ.Rst(i + 1); ++j) num_of_tr += SQ.Val(j);
+        nums[i] = num_of_tr >> 1;
+    }
+}
+
+// Restatement of triangle_counting_masked_lu (src/main.cpp:42-66) without the
+// stdout lines: C<A> = L·U with L = tril(A), U = transpose(L); sum(C) >> 1.
+int64_t tc_lu(const spMtx<int> &A, mxmOp<int> matrixMult, bool isParallel) {
+    int64_t num_of_tr = 0;
+    spMtx<int> L = std::move(extract_lower_triangle(A));
+    spMtx<int> U = std::move(transpose(L));
+    spMtx<int> C;
+    matrixMult(isParallel, L, U, A, C);
+    for (int j = 0; j < C.Rst(C.m); ++j) num_of_tr += C.Val(j);
+    return num_of_tr >> 1;
+}
+
 // Restatement of k_truss (src/main.cpp:94-141) without the stdout lines.
 // The one change: tmp_Xdj has n+1 entries (the reference sizes it n at
 // main.cpp:99 but writes index n at :118 and deep-copies it into an n+1
@@ -154,6 +178,30 @@ int ref_tc_sandia(int accum, int parallel, int64_t m, const int64_t *rp, const i
         if (!op) return -2;
         spMtx<int> A = make_mtx(m, m, rp, col, nullptr);
         *out = tc_sandia(A, op, parallel != 0);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_tc_vertex(int accum, int parallel, int64_t m, const int64_t *rp, const int32_t *col, int32_t *out) {
+    try {
+        mxmOp<int> op = pick(accum);
+        if (!op) return -2;
+        spMtx<int> A = make_mtx(m, m, rp, col, nullptr);
+        tc_vertex(A, op, parallel != 0, out);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+int ref_tc_lu(int accum, int parallel, int64_t m, const int64_t *rp, const int32_t *col, int64_t *out) {
+    try {
+        mxmOp<int> op = pick(accum);
+        if (!op) return -2;
+        spMtx<int> A = make_mtx(m, m, rp, col, nullptr);
+        *out = tc_lu(A, op, parallel != 0);
         return 0;
     } catch (...) {
         return -1;

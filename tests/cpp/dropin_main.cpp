@@ -51,10 +51,17 @@ int main(int argc, char **argv) {
     const bool symm_ok = (S == A);
     spMtx<int> AT = transpose(A);
     const bool transpose_ok = (AT.nz == A.nz);
+    int *per_vertex = triangle_counting_vertex(A, mxmm_msa<int, int>, true);
+    long long vertex_sum = 0;
+    for (size_t i = 0; i < A.m; ++i) vertex_sum += per_vertex[i];
+    delete[] per_vertex;
+    const int64_t tc_lu = triangle_counting_masked_lu(A, mxmm_msa<int, int>, true);
     std::printf("{\"scale\": %d, \"seed\": %llu, \"nnz\": %zu, \"tc_msa\": %lld, \"tc_mca\": %lld, \"tc_user\": %lld, "
                 "\"mxm_sum\": %lld, \"ktruss_nnz\": %zu, \"ktruss_iters\": %d, \"bc_float_sum\": %.9g, "
-                "\"bc_f64_sum\": %.17g, \"symm_roundtrip\": %s, \"transpose_nnz\": %s}\n",
+                "\"bc_f64_sum\": %.17g, \"symm_roundtrip\": %s, \"transpose_nnz\": %s, \"vertex_sum\": %lld, "
+                "\"tc_lu\": %lld}\n",
                 scale, (unsigned long long)seed, A.nz, (long long)tc_msa, (long long)tc_mca, (long long)tc_user,
-                csum, T.nz, iters, bcsum, bcdsum, symm_ok ? "true" : "false", transpose_ok ? "true" : "false");
+                csum, T.nz, iters, bcsum, bcdsum, symm_ok ? "true" : "false", transpose_ok ? "true" : "false",
+                vertex_sum, (long long)tc_lu);
     return 0;
 }

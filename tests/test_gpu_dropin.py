@@ -39,3 +39,5 @@ def test_dropin_matches_oracle(dropin_exe, gk, orc, cuda, scale, seed):
     assert res["bc_f64_sum"] == pytest.approx(bc.sum(), rel=1e-12)
     assert res["bc_float_sum"] == pytest.approx(bc.sum(), rel=1e-5)
     assert res["symm_roundtrip"] and res["transpose_nnz"]
+    assert res["tc_lu"] == tri
+    assert res["vertex_sum"] == int(orc.ref_tc_vertex(A).astype(np.int64).sum())

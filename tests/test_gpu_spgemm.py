@@ -209,3 +209,19 @@ def test_learned_without_model_is_an_error(gk, cuda):
     with pytest.raises(gk.GkError) as e:
         gk.tc_count(L, sched="learned")
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("scale,seed", [(9, 1), (11, 3), (13, 2)])
+def test_tc_vertex_and_lu_match_reference(gk, orc, cuda, scale, seed):
+    """Per-vertex triangle counts (C<A> = A·A row sums / 2) and the L·U count
+    against the reference's own triangle_counting_vertex / _masked_lu."""
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    want_v = orc.ref_tc_vertex(A) if scale < 13 else orc.tc_vertex(A)
+    got_v = gk.tc_vertex(dev(A)).cpu().numpy()
+    np.testing.assert_array_equal(got_v, want_v)
+    np.testing.assert_array_equal(gk.tc_vertex(A), want_v)  # host arrays
+    want = orc.ref_tc_lu(A) if scale < 13 else orc.tc_lower(gk.lower_host(A))
+    assert gk.tc_count_lu(dev(A)) == want == gk.tc_count(gk.lower_host(A))
+    from graphkokkos_b200 import sched
+    sched.load_model()
+    assert gk.tc_count_lu(dev(A), sched="learned") == want

@@ -120,6 +120,26 @@ def test_tc_vs_reference(gk, orc, scale, seed):
     assert orc.ref_tc(A, "mca", parallel=False) == got
 
 
+@pytest.mark.parametrize("scale,seed", [(8, 1), (10, 2), (12, 3)])
+def test_tc_vertex_and_lu_vs_reference(gk, orc, scale, seed):
+    """triangle_counting_vertex (src/main.cpp:16-39) and _masked_lu (:42-66)
+    of the reference (msa and mca) against the restatement."""
+    need_ref(orc)
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    want = orc.tc_vertex(A)
+    np.testing.assert_array_equal(orc.ref_tc_vertex(A, accum=0), want)
+    np.testing.assert_array_equal(orc.ref_tc_vertex(A, accum=1), want)
+    tri = orc.tc_lower(gk.lower_host(A))
+    assert int(want.astype(np.int64).sum()) == 3 * tri
+    assert orc.ref_tc_lu(A, accum=0) == orc.ref_tc_lu(A, accum=1) == tri
+
+
+def test_tc_vertex_closed_forms(orc):
+    for n in (4, 6, 9):  # every vertex of K_n lies in C(n-1, 2) triangles
+        np.testing.assert_array_equal(orc.tc_vertex(G.complete(n)), np.full(n, (n - 1) * (n - 2) // 2))
+    np.testing.assert_array_equal(orc.tc_vertex(G.star(6)), np.zeros(7))
+
+
 def test_mxmm_vs_reference(gk, orc):
     need_ref(orc)
     for seed in range(3):
