@@ -99,6 +99,10 @@ SIGNATURES = {
     "gk_host_graph_info": (ctypes.c_int, [VP, c_i64p, c_i64p]),
     "gk_host_graph_copy": (ctypes.c_int, [VP, VP, VP]),
     "gk_host_graph_free": (None, [VP]),
+    "gk_read_matrix": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(VP)]),
+    "gk_write_matrix": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(GkCsr)]),
+    "gk_host_graph_values": (ctypes.c_int, [VP, VP, c_i64p]),
+    "gk_host_graph_sort_rows": (ctypes.c_int, [VP]),
     "gk_sched_num_variants": (ctypes.c_int, []),
     "gk_sched_num_features": (ctypes.c_int, []),
     "gk_sched_model_size": (ctypes.c_size_t, []),

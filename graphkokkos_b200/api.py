@@ -349,6 +349,44 @@ def _take_host_graph(lib, h) -> Csr:
     return Csr(int(m.value), int(m.value), rp, col, None, int(nnz.value))
 
 
+FILE_FORMATS = {"auto": 0, "mtx": 1, "bin": 2, "crs": 3, "graph": 4, "rmat": 5}
+
+
+def read_matrix(path, fmt="auto", sort=False) -> Csr:
+    """Reads a matrix file in one of the reference's formats (mtx, bin, crs,
+    graph, rmat; include/matrix.h:44-60) into a host CSR.  Rows keep the
+    file's order, as the reference builds them; sort=True sorts every row's
+    columns, which the products and algorithms here require.  The values are
+    None for pattern files."""
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    check(lib.gk_read_matrix(str(path).encode(), FILE_FORMATS[fmt], ctypes.byref(h)))
+    if sort:
+        check(lib.gk_host_graph_sort_rows(h))
+    m = ctypes.c_int64(0)
+    nnz = ctypes.c_int64(0)
+    n = ctypes.c_int64(0)
+    lib.gk_host_graph_info(h, ctypes.byref(m), ctypes.byref(nnz))
+    rp = np.empty(m.value + 1, dtype=np.int64)
+    col = np.empty(nnz.value, dtype=np.int32)
+    val = np.empty(nnz.value, dtype=np.int32)
+    lib.gk_host_graph_copy(h, rp.ctypes.data, col.ctypes.data if nnz.value else None)
+    has = lib.gk_host_graph_values(h, val.ctypes.data if nnz.value else None, ctypes.byref(n))
+    lib.gk_host_graph_free(h)
+    return Csr(int(m.value), int(n.value), rp, col, val if has == 1 else None, int(nnz.value))
+
+
+def write_matrix(path, A: Csr, fmt="auto"):
+    """Writes a host CSR as MatrixMarket (mtx) or binary CSR (bin)."""
+    lib = _lib.load()
+    H = A.to(None) if _is_torch(A.rowptr) else A
+    rp = np.ascontiguousarray(np.asarray(H.rowptr, dtype=np.int64))
+    col = np.ascontiguousarray(np.asarray(H.col, dtype=np.int32))
+    val = None if H.val is None else np.ascontiguousarray(np.asarray(H.val, dtype=np.int32))
+    g = GkCsr(H.m, H.n, H.nnz, _ptr(rp), _ptr(col), _ptr(val))
+    check(lib.gk_write_matrix(str(path).encode(), FILE_FORMATS[fmt], ctypes.byref(g)))
+
+
 def lower_host(A: Csr) -> Csr:
     """Strict lower triangle of a host CSR with numpy (input preparation)."""
     rp = np.asarray(A.rowptr)

@@ -5,7 +5,10 @@
 
 struct gk_host_graph {
     int64_t m = 0;
+    int64_t n = 0;  // columns (0: square, n = m)
     int64_t nnz = 0;
     std::vector<int64_t> rp;
     std::vector<int32_t> col;
+    std::vector<int32_t> val;  // read from a file that carries values (has_val)
+    bool has_val = false;
 };

@@ -189,6 +189,33 @@ int gk_host_graph_info(const gk_host_graph *g, int64_t *m, int64_t *nnz);
 int gk_host_graph_copy(const gk_host_graph *g, int64_t *rowptr, int32_t *col);
 void gk_host_graph_free(gk_host_graph *g);
 
+/* ----- sparse-matrix files (host memory) ------------------------------------ */
+
+/* The reference's file formats (spMtx(const char *filename, format),
+ * include/matrix.h:44-60): GK_FILE_AUTO picks by the file's extension. */
+typedef enum gk_file_format {
+    GK_FILE_AUTO = 0,
+    GK_FILE_MTX = 1,    /* MatrixMarket coordinate (read_mtx_to_crs, matrix.h:259-395) */
+    GK_FILE_BIN = 2,    /* binary CSR (read_bin_to_crs, matrix.h:418-456) */
+    GK_FILE_CRS = 3,    /* text CSR (read_crs_to_crs, matrix.h:397-416) */
+    GK_FILE_GRAPH = 4,  /* adjacency lines (read_graph_to_crs, matrix.h:458-486) */
+    GK_FILE_RMAT = 5    /* edge pairs, symmetrised (read_rmat_to_crs, matrix.h:488-533) */
+} gk_file_format;
+
+/* Reads a matrix into a host graph handle (rows in the file's order, as the
+ * reference builds them; see gk_host_graph_sort_rows).  Errors: GK_ERR_ARG
+ * with gk_last_error_string(). */
+int gk_read_matrix(const char *path, int format, gk_host_graph **out);
+/* Writes A (host arrays) as mtx or bin; the bin layout is the reader's (the
+ * reference's write_crs_to_bin, matrix.h:210-227, stores Rst in place of Col
+ * and Val). */
+int gk_write_matrix(const char *path, int format, const gk_csr *A);
+/* Values of a handle: 1 and val[nnz] filled when the file carried values, 0
+ * for a pattern (values 1); *n receives the column count. */
+int gk_host_graph_values(const gk_host_graph *g, int32_t *val, int64_t *n);
+/* Sorts the columns of every row (values alongside, stable). */
+int gk_host_graph_sort_rows(gk_host_graph *g);
+
 /* ----- scheduler ------------------------------------------------------------ */
 
 /* Number of kernel variants the scheduler chooses among, and of the per-bin

@@ -237,6 +237,26 @@ def ref_ktruss(A_sym, k, accum="msa", parallel=True):
     return orp, ocol[: nnz.value].copy(), int(iters.value)
 
 
+def ref_read_matrix(path, fmt):
+    """The reference's reader for `fmt` (mtx, crs, bin, graph, rmat): a CSR
+    with the reference's Rst / Col / Val, or None if it cannot read the file."""
+    m, n, nz = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+    f = ref().ref_read_matrix
+    if f(str(path).encode(), fmt.encode(), ctypes.byref(m), ctypes.byref(n), ctypes.byref(nz), None, None, None) != 0:
+        return None
+    rp = np.zeros(m.value + 1, dtype=np.int64)
+    col = np.zeros(nz.value, dtype=np.int32)
+    val = np.zeros(nz.value, dtype=np.int32)
+    f(str(path).encode(), fmt.encode(), ctypes.byref(m), ctypes.byref(n), ctypes.byref(nz), _p(rp), _p(col), _p(val))
+
+    class _C:
+        pass
+
+    c = _C()
+    c.m, c.n, c.nnz, c.rowptr, c.col, c.val = int(m.value), int(n.value), int(nz.value), rp, col, val
+    return c
+
+
 def ref_tc_vertex(A, accum=0, parallel=True):
     """The reference's triangle_counting_vertex (src/main.cpp:16-39), restated
     around its mxmm_msa / mxmm_mca."""

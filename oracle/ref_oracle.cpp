@@ -184,6 +184,27 @@ int ref_tc_sandia(int accum, int parallel, int64_t m, const int64_t *rp, const i
     }
 }
 
+// The reference's file readers (spMtx(const char *, format), matrix.h:44-60):
+// call with null arrays for the sizes, then with arrays of those sizes.
+int ref_read_matrix(const char *path, const char *format, int64_t *m, int64_t *n, int64_t *nz, int64_t *rp,
+                    int32_t *col, int32_t *val) {
+    try {
+        spMtx<int> A(path, std::string(format));
+        *m = static_cast<int64_t>(A.m);
+        *n = static_cast<int64_t>(A.n);
+        *nz = static_cast<int64_t>(A.nz);
+        if (rp)
+            for (size_t i = 0; i <= A.m; ++i) rp[i] = A.Rst(i);
+        if (col)
+            for (size_t j = 0; j < A.nz; ++j) col[j] = A.Col(j);
+        if (val)
+            for (size_t j = 0; j < A.nz; ++j) val[j] = A.Val(j);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
 int ref_tc_vertex(int accum, int parallel, int64_t m, const int64_t *rp, const int32_t *col, int32_t *out) {
     try {
         mxmOp<int> op = pick(accum);
