@@ -84,6 +84,7 @@ SIGNATURES = {
     "gk_mxmm_masked_variant": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 3 + [VP, ctypes.c_int, ctypes.c_int, VP]),
     "gk_tc_row_sums": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
     "gk_tc_vertex": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
+    "gk_mxmm_cmask": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 3 + [ctypes.c_int, VP, VP, VP, VP]),
     "gk_tc_count_lu": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
     "gk_tc_count_batched": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, ctypes.c_int, VP]),
     "gk_ktruss": (ctypes.c_int, [ctypes.POINTER(GkCsrMut), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, VP]),

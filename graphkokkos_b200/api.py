@@ -172,6 +172,24 @@ def tc_row_sums(L: Csr, sched="plain", stream=None):
     return out
 
 
+def mxmm_cmask(A: Csr, B: Csr, M: Csr, semiring="plus_times", stream=None) -> Csr:
+    """C<!M> = A·B (mxmm_msa_cmask, include/matrix_la.h:733-934): C's entries
+    are the columns a product reaches that are not in M's row; sorted rows.
+    Returned in the memory space of A."""
+    lib = _lib.load()
+    sr = {"plus_times": 0, "plus_pair": 1}[semiring]
+    ga, gb, gm = A.as_gk(), B.as_gk(), M.as_gk()
+    st = _stream(stream, A.col)
+    rp = _empty_like_space(A.rowptr, (A.m + 1,), np.int64)
+    check(lib.gk_mxmm_cmask(ctypes.byref(ga), ctypes.byref(gb), ctypes.byref(gm), sr, _ptr(rp), None, None, st))
+    nnz = int(rp[-1])
+    col = _empty_like_space(A.col, (max(nnz, 1),), np.int32)
+    val = _empty_like_space(A.col, (max(nnz, 1),), np.int32)
+    check(lib.gk_mxmm_cmask(ctypes.byref(ga), ctypes.byref(gb), ctypes.byref(gm), sr, _ptr(rp), _ptr(col), _ptr(val),
+                            st))
+    return Csr(A.m, B.n, rp, col[:nnz], val[:nnz], nnz)
+
+
 def tc_vertex(A: Csr, sched="plain", stream=None):
     """Triangles through each vertex of a symmetric adjacency
     (triangle_counting_vertex, src/main.cpp:16-39); int32 per vertex."""

@@ -10,6 +10,7 @@
 //   mxmm_msa / mxmm_mca / mxmm_naive / mxmm_gpu
 //                       include/matrix_la.h:478-694, :936-1068 — C<M> = A·B, C
 //                       resized to M's pattern with explicit zeros kept (:564-568)
+//   mxmm_msa_cmask      include/matrix_la.h:733-934 — C<!M> = A·B
 //   triangle_counting_masked_sandia   src/main.cpp:69-90
 //   triangle_counting_vertex          src/main.cpp:16-39
 //   triangle_counting_masked_lu       src/main.cpp:42-66
@@ -188,6 +189,21 @@ void mxmm_naive(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, s
 template <typename T>
 void mxmm_gpu(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, spMtx<T> &C) {
     gkb_detail::mxmm_with(GK_ACCUM_AUTO, A, B, M, C);
+}
+
+// Complement-masked product C<!M> = A·B (include/matrix_la.h:733-934): C is
+// resized to the product's pattern minus M's, rows sorted.
+template <typename T, typename U>
+void mxmm_msa_cmask(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &M, spMtx<T> &C) {
+    static_assert(std::is_same<T, int>::value, "the GPU operators take int matrices (spMtx<int>)");
+    gk_csr a = A.csr(), b = B.csr();
+    gk_csr mm{static_cast<int64_t>(M.m), static_cast<int64_t>(M.n), static_cast<int64_t>(M.nz), M.Rst.data(),
+              M.Col.data(), nullptr};
+    spMtx<T> R(M.m, M.n);
+    gkb_detail::check(gk_mxmm_cmask(&a, &b, &mm, GK_PLUS_TIMES, R.Rst.data(), nullptr, nullptr, nullptr));
+    R.resizeVals(static_cast<size_t>(R.Rst(M.m)));
+    gkb_detail::check(gk_mxmm_cmask(&a, &b, &mm, GK_PLUS_TIMES, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
+    C = R;
 }
 
 // ----- CSR transforms ------------------------------------------------------------

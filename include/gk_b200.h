@@ -118,6 +118,18 @@ int gk_tc_count_noalloc(const gk_csr *L, uint64_t *count, int sched, void *strea
  * triangle_counting_vertex, src/main.cpp:16-39). */
 int gk_tc_row_sums(const gk_csr *L, uint64_t *row_sums, int sched, void *stream);
 
+/* Complement-masked product C<!M> = A·B (mxmm_msa_cmask,
+ * include/matrix_la.h:733-934): row i of C holds every column reached by a
+ * product A(i,k)·B(k,j) that is not a column of M's row i, in ascending
+ * order (kept even where the sum is zero), with the sum of the products
+ * (PLUS_TIMES; PLUS_PAIR counts them).  Unlike gk_mxmm_masked, C's pattern
+ * is not known in advance, so two calls, as the reference's symbolic and
+ * numeric passes: with C_col == NULL, C_rowptr (A.m + 1 entries) receives the
+ * row pointers; then, with C_rowptr from that call and C_col / C_val of
+ * C_rowptr[A.m] entries (C_val may be NULL), the columns and values. */
+int gk_mxmm_cmask(const gk_csr *A, const gk_csr *B, const gk_csr *M, int semiring, int64_t *C_rowptr,
+                  int32_t *C_col, int32_t *C_val, void *stream);
+
 /* Triangles through each vertex of a symmetric adjacency A:
  * counts[i] = (sum_j C(i,j)) >> 1 with C<A> = A·A, as int like the reference's
  * triangle_counting_vertex (src/main.cpp:16-39).  counts has A.m entries. */

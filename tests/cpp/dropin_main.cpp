@@ -56,12 +56,16 @@ int main(int argc, char **argv) {
     for (size_t i = 0; i < A.m; ++i) vertex_sum += per_vertex[i];
     delete[] per_vertex;
     const int64_t tc_lu = triangle_counting_masked_lu(A, mxmm_msa<int, int>, true);
+    spMtx<int> NC;  // two-hop pairs that are not edges: C<!A> = A·A
+    mxmm_msa_cmask(true, A, A, A, NC);
+    long long ncsum = 0;
+    for (size_t j = 0; j < NC.nz; ++j) ncsum += NC.Val(j);
     std::printf("{\"scale\": %d, \"seed\": %llu, \"nnz\": %zu, \"tc_msa\": %lld, \"tc_mca\": %lld, \"tc_user\": %lld, "
                 "\"mxm_sum\": %lld, \"ktruss_nnz\": %zu, \"ktruss_iters\": %d, \"bc_float_sum\": %.9g, "
                 "\"bc_f64_sum\": %.17g, \"symm_roundtrip\": %s, \"transpose_nnz\": %s, \"vertex_sum\": %lld, "
-                "\"tc_lu\": %lld}\n",
+                "\"tc_lu\": %lld, \"cmask_nnz\": %zu, \"cmask_sum\": %lld}\n",
                 scale, (unsigned long long)seed, A.nz, (long long)tc_msa, (long long)tc_mca, (long long)tc_user,
                 csum, T.nz, iters, bcsum, bcdsum, symm_ok ? "true" : "false", transpose_ok ? "true" : "false",
-                vertex_sum, (long long)tc_lu);
+                vertex_sum, (long long)tc_lu, NC.nz, ncsum);
     return 0;
 }

@@ -40,4 +40,6 @@ def test_dropin_matches_oracle(dropin_exe, gk, orc, cuda, scale, seed):
     assert res["bc_float_sum"] == pytest.approx(bc.sum(), rel=1e-5)
     assert res["symm_roundtrip"] and res["transpose_nnz"]
     assert res["tc_lu"] == tri
+    crp, ccol, cval = orc.mxmm_cmask(A, A, A)
+    assert res["cmask_nnz"] == len(ccol) and res["cmask_sum"] == int(cval.astype(np.int64).sum())
     assert res["vertex_sum"] == int(orc.ref_tc_vertex(A).astype(np.int64).sum())
