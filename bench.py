@@ -384,8 +384,8 @@ def bc_traversed(A, src):
     (the TEPS numerator), and the directed edges of those components."""
     import scipy.sparse as sp
     import scipy.sparse.csgraph as cg
-    rp = A.rowptr.cpu().numpy()
-    col = A.col.cpu().numpy()
+    rp = A.rowptr.cpu().numpy() if hasattr(A.rowptr, "cpu") else np.asarray(A.rowptr)
+    col = A.col.cpu().numpy() if hasattr(A.col, "cpu") else np.asarray(A.col)
     M = sp.csr_matrix((np.ones(len(col), dtype=np.int8), col, rp), shape=(A.m, A.m))
     ncomp, lab = cg.connected_components(M, directed=False)
     directed_per_comp = np.bincount(lab[np.repeat(np.arange(A.m), np.diff(rp))], minlength=ncomp)
@@ -609,6 +609,73 @@ def main_ours(args):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU code on this host's cores
 # ---------------------------------------------------------------------------
+def reference_line(args, wl, world, value, unit, config, kind, cores, sample):
+    return {"metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32" if unit != "TEPS" else "f32", "data": "synthetic",
+            "impl": "reference", "config": config,
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def reference_bc(args, wl, world):
+    """The reference's betweenness_centrality_batch (oracle/_ref) on a few of
+    the workload's sources per step (relabelled to 0..b-1, as it takes them),
+    one thread (its row split is unsafe with more)."""
+    import oracle
+    import graphkokkos_b200 as gk
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled here) not built"}))
+        return
+    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"])
+    src = np.random.default_rng(wl["src_seed"]).choice(A.m, size=wl["nsrc"], replace=False)
+    per = 4
+    vals = []
+    for i in range(args.warmup + args.steps):
+        pick = src[(per * i) % len(src):(per * i) % len(src) + per]
+        R, _ = oracle.relabel_sources_first(A, pick)
+        t0 = time.perf_counter()
+        oracle.ref_bc_float(R, len(pick), threads=1)
+        sec = time.perf_counter() - t0
+        trav, _ = bc_traversed(A, pick)
+        if i >= args.warmup:
+            vals.append(trav / sec)
+    v = statistics.median(vals)
+    print(json.dumps(reference_line(
+        args, wl, world, v, "TEPS",
+        {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources", "sched": "n/a"},
+        "reference", 1, f"each step: {per} of the workload's sources, reference BC (float), one thread")))
+
+
+def reference_tcbatch(args, wl, world):
+    """The reference's triangle count (mxmm_msa, oracle/_ref) on whole graphs
+    of the batch, a different slice of graphs per step, on the host's cores."""
+    import oracle
+    import graphkokkos_b200 as gk
+    kind = "reference" if oracle.ref_available() else "port"
+    specs = gk.api.uneven_batch_specs(wl["ngraphs"], wl["seed0"])
+    vals = []
+    thr = 1
+    for i in range(args.warmup + args.steps):
+        nz_tot, sec_tot = 0, 0.0
+        for g in range(i, len(specs), 97):
+            kind_g, a, b, seed = specs[g]
+            A = gk.gen_rmat(a, b, seed=seed) if kind_g == "rmat" else gk.gen_er(a, b, seed=seed)
+            _, nz, sec, thr = oracle.tc_row_stride(gk.lower_host(A), 1, 0, kind=kind)
+            nz_tot += nz
+            sec_tot += sec
+            if sec_tot > max(2.0, 120.0 / max(1, args.steps + args.warmup)):
+                break
+        if i >= args.warmup:
+            vals.append(nz_tot / sec_tot)
+    v = statistics.median(vals)
+    print(json.dumps(reference_line(
+        args, wl, world, v, "edges/s",
+        {"workload": f"many-graph triangle counting, {wl['ngraphs']} graphs", "sched": "n/a"},
+        kind, thr, "each step: whole graphs g = step, step+97, ... of the batch until ~the step's time budget; "
+                   "the reference's mxmm_msa + sum per graph")))
+
+
 def main_reference(args):
     rank, _, world = rank_info()
     if rank != 0:
@@ -616,8 +683,14 @@ def main_reference(args):
     import oracle
     import graphkokkos_b200 as gk
     wl = WORKLOADS[args.workload]
+    if wl["kind"] == "bc":
+        return reference_bc(args, wl, world)
+    if wl["kind"] == "tcbatch":
+        return reference_tcbatch(args, wl, world)
     if wl["kind"] != "tc":
-        print(json.dumps({"impl": "reference", "unavailable": "reference arm implemented for the tc workloads"}))
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "k-truss is not sampleable: the reference's whole loop on RMAT-20 takes tens of minutes "
+                          "on the host cores (11 passes of its support product)"}))
         return
     try:
         import torch
