@@ -46,6 +46,19 @@ __device__ __forceinline__ uint32_t filter_bit(int x) {
     return (static_cast<uint32_t>(x) * 0x85EBCA77u) >> (32 - FLOG);
 }
 
+// Position of x in a filter whose first 2^LOWB bits map columns below 2^LOWB
+// one to one (an exact bitmap of the low columns, where power-law graphs
+// without relabelling keep their hubs) followed by the 2^FLOG hashed bits.
+template <int FLOG, int LOWB>
+__device__ __forceinline__ uint32_t filter_pos(int x) {
+    if constexpr (LOWB > 0) {
+        const uint32_t ux = static_cast<uint32_t>(x);
+        return ux < (1u << LOWB) ? ux : (1u << LOWB) + filter_bit<FLOG>(x);
+    } else {
+        return filter_bit<FLOG>(x);
+    }
+}
+
 // The mask tables are bucketed open addressing: CAP slots as CAP/4 buckets
 // of four adjacent slots, read with one 16-byte shared-memory load.  A key
 // lives in its home bucket or, when that bucket is full, in the following

@@ -13,12 +13,13 @@
 //    entry's B-row bounds are loaded while the current B row streams.
 #pragma once
 
-template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL>
+template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL, int LOWB = 0>
 __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THREADS / NT)) k_block(KArgs p) {
     constexpr bool ACC = (EPI == EPI_WRITE);
     constexpr int NW = NT / 32;
     constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;  // MSA: CAP = log2 window width
-    constexpr int FWORDS = (KIND == K_HASH_BLOCK && FLOG > 0) ? (1 << FLOG) / 32 : 0;
+    // filter words: 2^LOWB exact bits for the low columns, then 2^FLOG hashed bits
+    constexpr int FWORDS = (KIND == K_HASH_BLOCK && FLOG > 0) ? ((1 << LOWB) + (1 << FLOG)) / 32 : 0;
     constexpr int PKV = (KIND == K_MSA_BLOCK) ? PK_MSA : ((KIND == K_MCA_BLOCK) ? PK_MCA : PK_HASH);
     extern __shared__ int smem[];
     __shared__ unsigned long long s_red[NW];
@@ -125,9 +126,11 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
                 __syncthreads();
                 for (int q = c0 + threadIdx.x; q < c1; q += NT) {
                     const int x = mc[q];
-                    hash_insert<CAP>(keys, x);
+                    // without accumulators a low column needs no slot: its
+                    // filter bit is exact
+                    if (ACC || LOWB == 0 || static_cast<uint32_t>(x) >= (1u << LOWB)) hash_insert<CAP>(keys, x);
                     if constexpr (FWORDS > 0) {
-                        const uint32_t h = filter_bit<FLOG>(x);
+                        const uint32_t h = filter_pos<FLOG, LOWB>(x);
                         atomicOr(filt + (h >> 5), 1u << (h & 31));
                     }
                 }
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
                             }
                         }
                         if (!skip)
-                            stream_row<SUB, CAP, PKV, ACC, VAL, (FWORDS > 0 ? FLOG : 0)>(
+                            stream_row<SUB, CAP, PKV, ACC, VAL, (FWORDS > 0 ? FLOG : 0), (FWORDS > 0 ? LOWB : 0)>(
                                 p, cur.b0, cur.b1, sl, cur.av, pkeys, acc, probe_arg, cnt, pfilt, hi_col);
                     }
                     tc = tn;

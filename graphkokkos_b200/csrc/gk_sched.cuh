@@ -44,9 +44,10 @@ struct Variant {
     int flog;       // block HASH kinds: log2 bits of the bitmap filter in front of the table
     int batch;      // items a CTA (group kinds: a warp) takes per fetch
     int accum;      // gk_accum family this variant belongs to
+    int lowb;       // block HASH kinds: log2 of the low-column range the filter maps exactly (0: none)
 };
 
-constexpr int NV = 15;
+constexpr int NV = 17;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
 // Tables are bucketed (four slots per 16-byte load).  The small ones run at
 // load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
@@ -54,23 +55,27 @@ constexpr int NV = 15;
 // entry) send only filter candidates to the table; variants 12-14 have none
 // and look every streamed element up in the table directly, which wins on
 // rows where a large share of the elements are mask columns.
-// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum
+// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum,
+// exact low-column bits (variants 15, 16: the filter maps columns below 2^lowb
+// one to one, so a hit there needs no table lookup when only sums are kept)
 #define GK_VARIANT_TABLE { \
-    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3},   \
-    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3},   \
-    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 13, 1, 3},   \
-    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3},   \
-    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
-    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3},   \
-    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 16, 2, 3},   \
-    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19, 17, 1, 3},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3},   \
-    {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2},   \
-    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2},   \
-    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1},   \
-    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3},   \
-    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18,  0, 2, 3},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3},   \
+    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3  , 0},   \
+    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3  , 0},   \
+    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 13, 1, 3  , 0},   \
+    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3  , 0},   \
+    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
+    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 16, 2, 3  , 0},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19, 17, 1, 3  , 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3  , 0},   \
+    {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2  , 0},   \
+    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2  , 0},   \
+    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1  , 0},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3  , 0},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18,  0, 2, 3  , 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3  , 0},   \
+    {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18},  \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 14, 2, 3  , 15},  \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -103,6 +108,8 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 12: return qm >= 5;
         case 13: return true;
         case 14: return qm >= 8;
+        case 15: return qm >= 8;
+        case 16: return true;
         default: return false;
     }
 }

@@ -227,14 +227,20 @@ enum : int { PK_HASH = 0, PK_MCA = 1, PK_MSA = 2 };
 // HASH  slot of x in a CAP-slot hash set;  MCA  position of x in the sorted
 // chunk keys[0, clen);  MSA  x - base if its bit is set in a 2^CAP-column
 // window bitmap (keys reinterpreted as words).
-template <int CAP, int PK, bool ACC, int FLOG = 0>
+template <int CAP, int PK, bool ACC, int FLOG = 0, int LOWB = 0>
 __device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, int *acc, int clen, unsigned &cnt,
                                            const unsigned *filt = nullptr) {
     int s;
     if constexpr (PK == PK_HASH && FLOG > 0) {
         // bitmap filter first: most B elements are not mask columns
-        const uint32_t h = filter_bit<FLOG>(x);
+        const uint32_t h = filter_pos<FLOG, LOWB>(x);
         if (!((filt[h >> 5] >> (h & 31)) & 1u)) return;
+        if constexpr (!ACC && LOWB > 0) {
+            if (static_cast<uint32_t>(x) < (1u << LOWB)) {  // exact part of the filter: a hit
+                cnt += w;
+                return;
+            }
+        }
     }
     if constexpr (PK == PK_MSA) {
         const int y = x - clen;  // clen carries the window base for MSA
@@ -253,9 +259,9 @@ __device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, i
 }
 
 // Filter bit of x (0/1) and the exact test of a filter candidate.
-template <int FLOG>
+template <int FLOG, int LOWB = 0>
 __device__ __forceinline__ uint32_t cand_bit(int x, const unsigned *filt) {
-    const uint32_t h = filter_bit<FLOG>(x);
+    const uint32_t h = filter_pos<FLOG, LOWB>(x);
     return (filt[h >> 5] >> (h & 31)) & 1u;
 }
 
@@ -273,7 +279,7 @@ __device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, i
 // (bit e of m set = element e passed the filter).  Each lane walks only its
 // own set bits, so a warp iterates as often as its busiest lane has
 // candidates instead of once per element position with a lane or two active.
-template <int CAP, bool ACC>
+template <int CAP, bool ACC, int LOWB = 0>
 __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int4 &y, uint32_t av,
                                             const int *keys, int *acc, unsigned &cnt) {
     while (m) {
@@ -281,7 +287,14 @@ __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int
         m &= m - 1;
         const int lo = (e & 1) ? ((e & 4) ? y.y : x.y) : ((e & 4) ? y.x : x.x);
         const int hi = (e & 1) ? ((e & 4) ? y.w : x.w) : ((e & 4) ? y.z : x.z);
-        exact_hash<CAP, ACC>((e & 2) ? hi : lo, av, keys, acc, cnt);
+        const int v = (e & 2) ? hi : lo;
+        if constexpr (!ACC && LOWB > 0) {
+            if (static_cast<uint32_t>(v) < (1u << LOWB)) {  // exact part of the filter: a hit
+                cnt += av;
+                continue;
+            }
+        }
+        exact_hash<CAP, ACC>(v, av, keys, acc, cnt);
     }
 }
 
@@ -291,7 +304,7 @@ __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int
 // filter without branches and only the candidates take the exact lookup.  A
 // lane stops once its elements pass hi_col, the last mask column of the
 // item (B rows are sorted); elements beyond it could never match.
-template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0>
+template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0, int LOWB = 0>
 __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b1, int sl, uint32_t av,
                                            const int *keys, int *acc, int clen, unsigned &cnt,
                                            const unsigned *filt, int hi_col) {
@@ -300,7 +313,7 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
         if (p.vec) {
             int64_t h1 = (b0 + 3) & ~int64_t(3);
             if (h1 > b1) h1 = b1;
-            if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
+            if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
             const int4 *__restrict__ base = reinterpret_cast<const int4 *>(bc) + (h1 >> 2);
             const int n4 = static_cast<int>((b1 >> 2) - (h1 >> 2));
             int q = sl;
@@ -308,11 +321,11 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             for (; q + SUB < n4; q += 2 * SUB) {
                 const int4 x = __ldg(base + q);
                 const int4 y = __ldg(base + q + SUB);
-                const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
-                                   (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3) |
-                                   (cand_bit<FLOG>(y.x, filt) << 4) | (cand_bit<FLOG>(y.y, filt) << 5) |
-                                   (cand_bit<FLOG>(y.z, filt) << 6) | (cand_bit<FLOG>(y.w, filt) << 7);
-                exact_cands<CAP, ACC>(m, x, y, av, keys, acc, cnt);
+                const uint32_t m = cand_bit<FLOG, LOWB>(x.x, filt) | (cand_bit<FLOG, LOWB>(x.y, filt) << 1) |
+                                   (cand_bit<FLOG, LOWB>(x.z, filt) << 2) | (cand_bit<FLOG, LOWB>(x.w, filt) << 3) |
+                                   (cand_bit<FLOG, LOWB>(y.x, filt) << 4) | (cand_bit<FLOG, LOWB>(y.y, filt) << 5) |
+                                   (cand_bit<FLOG, LOWB>(y.z, filt) << 6) | (cand_bit<FLOG, LOWB>(y.w, filt) << 7);
+                exact_cands<CAP, ACC, LOWB>(m, x, y, av, keys, acc, cnt);
                 if (y.w > hi_col) {  // B rows are sorted: the rest cannot be mask columns
                     past = true;
                     break;
@@ -320,20 +333,20 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             }
             if (!past && q < n4) {
                 const int4 x = __ldg(base + q);
-                const uint32_t m = cand_bit<FLOG>(x.x, filt) | (cand_bit<FLOG>(x.y, filt) << 1) |
-                                   (cand_bit<FLOG>(x.z, filt) << 2) | (cand_bit<FLOG>(x.w, filt) << 3);
-                exact_cands<CAP, ACC>(m, x, x, av, keys, acc, cnt);
+                const uint32_t m = cand_bit<FLOG, LOWB>(x.x, filt) | (cand_bit<FLOG, LOWB>(x.y, filt) << 1) |
+                                   (cand_bit<FLOG, LOWB>(x.z, filt) << 2) | (cand_bit<FLOG, LOWB>(x.w, filt) << 3);
+                exact_cands<CAP, ACC, LOWB>(m, x, x, av, keys, acc, cnt);
             }
             int64_t tl = (b1 >> 2) << 2;
             if (tl < h1) tl = h1;
-            if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
+            if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
             return;
         }
     }
     if (!VAL && p.vec) {
         int64_t h1 = (b0 + 3) & ~int64_t(3);
         if (h1 > b1) h1 = b1;
-        if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
+        if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
         const int64_t v1 = b1 >> 2;
         const int4 *__restrict__ bv = reinterpret_cast<const int4 *>(bc);
         int64_t q = (h1 >> 2) + sl;
@@ -341,14 +354,14 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
         for (; q + SUB < v1; q += 2 * SUB) {
             const int4 x = __ldg(bv + q);
             const int4 y = __ldg(bv + q + SUB);
-            probe_elem<CAP, PK, ACC, FLOG>(x.x, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.y, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.z, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.w, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(y.x, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(y.y, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(y.z, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(y.w, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.w, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(y.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(y.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(y.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(y.w, av, keys, acc, clen, cnt, filt);
             if (y.w > hi_col) {
                 past = true;
                 break;
@@ -356,21 +369,21 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
         }
         if (!past && q < v1) {
             const int4 x = __ldg(bv + q);
-            probe_elem<CAP, PK, ACC, FLOG>(x.x, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.y, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.z, av, keys, acc, clen, cnt, filt);
-            probe_elem<CAP, PK, ACC, FLOG>(x.w, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.x, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.y, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.z, av, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x.w, av, keys, acc, clen, cnt, filt);
         }
         int64_t tl = v1 << 2;
         if (tl < h1) tl = h1;
-        if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
+        if (tl + sl < b1) probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
     } else {
         const int32_t *__restrict__ bvals = VAL ? p.B.val : nullptr;
         for (int64_t j = b0 + sl; j < b1; j += SUB) {
             const int x = __ldg(bc + j);
             if (x > hi_col) break;
             const uint32_t w = (VAL && bvals) ? av * static_cast<uint32_t>(__ldg(bvals + j)) : av;
-            probe_elem<CAP, PK, ACC, FLOG>(x, w, keys, acc, clen, cnt, filt);
+            probe_elem<CAP, PK, ACC, FLOG, LOWB>(x, w, keys, acc, clen, cnt, filt);
         }
     }
 }
@@ -579,7 +592,8 @@ constexpr size_t smem_bytes(bool write) {
         return (size_t(1) << X.cap) / 8;
     } else {
         const int cap = write ? X.cap_write : X.cap;
-        const size_t filter = (X.kind == K_HASH_BLOCK && X.flog > 0) ? (size_t(1) << X.flog) / 8 : 0;
+        const size_t filter =
+            (X.kind == K_HASH_BLOCK && X.flog > 0) ? ((size_t(1) << X.lowb) + (size_t(1) << X.flog)) / 8 : 0;
         return size_t(cap) * 4 * (write ? 2 : 1) + filter;
     }
 }
@@ -603,7 +617,7 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         constexpr int CAPV = W ? X.cap_write : X.cap;
         constexpr int CHV = W ? X.chunk_write : X.chunk;
         constexpr int FLOGV = (X.kind == K_HASH_BLOCK) ? X.flog : 0;
-        fn = k_block<X.G, X.kind, X.sub, CAPV, CHV, X.split_log2, FLOGV, X.batch, EPI, VAL>;
+        fn = k_block<X.G, X.kind, X.sub, CAPV, CHV, X.split_log2, FLOGV, X.batch, EPI, VAL, (FLOGV > 0 ? X.lowb : 0)>;
         nt = X.G;
     }
     // resident CTAs per SM, computed once per kernel instance (and device)
@@ -650,6 +664,8 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 12: return launch_variant_v<12>(a, epi, val, sms, s, launch);
         case 13: return launch_variant_v<13>(a, epi, val, sms, s, launch);
         case 14: return launch_variant_v<14>(a, epi, val, sms, s, launch);
+        case 15: return launch_variant_v<15>(a, epi, val, sms, s, launch);
+        case 16: return launch_variant_v<16>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
 }
