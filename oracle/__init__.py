@@ -139,6 +139,32 @@ def mxmm(A, B, M):
     return out
 
 
+def _cmask(fn, A, B, M, *extra):
+    am, an, arp, acol, aval = _host(A)
+    bm, bn, brp, bcol, bval = _host(B)
+    mm, mn, mrp, mcol, _ = _host(M)
+    rp = np.zeros(am + 1, dtype=np.int64)
+    args = (I64(am), I64(an), _p(arp), _p(acol), _p(aval), I64(bm), I64(bn), _p(brp), _p(bcol), _p(bval),
+            I64(mm), I64(mn), _p(mrp), _p(mcol))
+    if fn(*extra, *args, _p(rp), None, None) != 0:
+        raise ValueError("complement-masked product failed")
+    col = np.zeros(int(rp[-1]), dtype=np.int32)
+    val = np.zeros(int(rp[-1]), dtype=np.int32)
+    if fn(*extra, *args, _p(rp), _p(col), _p(val)) != 0:
+        raise ValueError("complement-masked product failed")
+    return rp, col, val
+
+
+def mxmm_cmask(A, B, M):
+    """C<!M> = A·B (mxmm_msa_cmask semantics): (rowptr, col, val)."""
+    return _cmask(port().orc_mxmm_cmask, A, B, M)
+
+
+def ref_mxmm_cmask(A, B, M, parallel=True):
+    """The reference's own mxmm_msa_cmask (matrix_la.h:733-934)."""
+    return _cmask(ref().ref_mxmm_cmask, A, B, M, ctypes.c_int(1 if parallel else 0))
+
+
 def ktruss(A, k, record=64):
     m, _, rp, col, _ = _host(A)
     orp = np.zeros(m + 1, dtype=np.int64)

@@ -124,6 +124,61 @@ int orc_mxmm_masked(int64_t am, int64_t an, const int64_t *arp, const int32_t *a
     return 0;
 }
 
+// Complement-masked product C<!M> = A·B (mxmm_msa_cmask, matrix_la.h:733-934):
+// row i of C holds every column j reached by some A(i,k)·B(k,j) (structurally,
+// whatever the sum) that is not a column of M's row i, in ascending order,
+// with the wrapping int32 sum of the products.  Two calls: c_col == nullptr
+// fills c_rp (m+1) only; then c_col / c_val of c_rp[m] entries.
+int orc_mxmm_cmask(int64_t am, int64_t an, const int64_t *arp, const int32_t *acol, const int32_t *aval,
+                   int64_t bm, int64_t bn, const int64_t *brp, const int32_t *bcol, const int32_t *bval,
+                   int64_t mm, int64_t mn, const int64_t *mrp, const int32_t *mcol,
+                   int64_t *c_rp, int32_t *c_col, int32_t *c_val) {
+    if (am != mm || an != bm || bn != mn) return -1;
+    Csr A{am, an, arp, acol, aval}, B{bm, bn, brp, bcol, bval};
+    std::vector<int64_t> cnt(static_cast<size_t>(am), 0);
+#pragma omp parallel
+    {
+        std::vector<uint8_t> state(static_cast<size_t>(bn), 0);  // 0 free, 1 masked, 2 reached
+        std::vector<uint32_t> accum(static_cast<size_t>(bn), 0u);
+        std::vector<int32_t> touched;
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < am; ++i) {
+            for (int64_t j = mrp[i]; j < mrp[i + 1]; ++j) state[mcol[j]] = 1;
+            for (int64_t t = A.rp[i]; t < A.rp[i + 1]; ++t) {
+                const int32_t k = A.col[t];
+                const uint32_t a = static_cast<uint32_t>(A.v(t));
+                for (int64_t j = B.rp[k]; j < B.rp[k + 1]; ++j) {
+                    const int32_t c = B.col[j];
+                    if (state[c] == 1) continue;
+                    if (state[c] == 0) {
+                        state[c] = 2;
+                        accum[c] = 0u;
+                        touched.push_back(c);
+                    }
+                    accum[c] += a * static_cast<uint32_t>(B.v(j));
+                }
+            }
+            std::sort(touched.begin(), touched.end());
+            cnt[i] = static_cast<int64_t>(touched.size());
+            if (c_col) {
+                int64_t p = c_rp[i];
+                for (int32_t c : touched) {
+                    c_col[p] = c;
+                    c_val[p++] = static_cast<int32_t>(accum[c]);
+                }
+            }
+            for (int32_t c : touched) state[c] = 0;
+            touched.clear();
+            for (int64_t j = mrp[i]; j < mrp[i + 1]; ++j) state[mcol[j]] = 0;
+        }
+    }
+    if (!c_col) {
+        c_rp[0] = 0;
+        for (int64_t i = 0; i < am; ++i) c_rp[i + 1] = c_rp[i] + cnt[i];
+    }
+    return 0;
+}
+
 // Triangle count from the strict lower triangle L: sum of C<L> = L·L
 // (triangle_counting_masked_sandia, src/main.cpp:69-90) restricted to rows
 // [row_begin, row_end) of A and M (B = all of L).  Counting form of the MSA

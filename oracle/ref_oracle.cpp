@@ -171,6 +171,31 @@ int ref_mxmm(int accum, int parallel,
     }
 }
 
+// The reference's complement-masked product mxmm_msa_cmask (matrix_la.h:733-934).
+// Two calls as orc_mxmm_cmask: c_col == nullptr gives c_rp only.
+int ref_mxmm_cmask(int parallel,
+                   int64_t am, int64_t an, const int64_t *arp, const int32_t *acol, const int32_t *aval,
+                   int64_t bm, int64_t bn, const int64_t *brp, const int32_t *bcol, const int32_t *bval,
+                   int64_t mm, int64_t mn, const int64_t *mrp, const int32_t *mcol,
+                   int64_t *c_rp, int32_t *c_col, int32_t *c_val) {
+    try {
+        spMtx<int> A = make_mtx(am, an, arp, acol, aval);
+        spMtx<int> B = make_mtx(bm, bn, brp, bcol, bval);
+        spMtx<int> M = make_mtx(mm, mn, mrp, mcol, nullptr);
+        spMtx<int> C;
+        mxmm_msa_cmask(parallel != 0, A, B, M, C);
+        for (size_t i = 0; i <= C.m; ++i) c_rp[i] = C.Rst(i);
+        if (c_col)
+            for (size_t j = 0; j < C.nz; ++j) {
+                c_col[j] = C.Col(j);
+                c_val[j] = C.Val(j);
+            }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
 // Triangle count of a symmetric adjacency matrix (sorted rows, no self-loops).
 int ref_tc_sandia(int accum, int parallel, int64_t m, const int64_t *rp, const int32_t *col, int64_t *out) {
     try {

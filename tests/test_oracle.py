@@ -244,3 +244,22 @@ def test_golden_bc(gk, orc):
         ours = orc.bc_f64(A, src)
         ref = np.asarray(case["bc_ref_float"], dtype=np.float64)
         np.testing.assert_allclose(ours, ref, rtol=2e-4, atol=1e-2)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_cmask_vs_reference(orc, seed):
+    """mxmm_msa_cmask (include/matrix_la.h:733-934): the restatement gives the
+    reference's C<!M> = A·B entry for entry, values included, on rectangular
+    operands and on the two-hop non-edges of a graph (A, A, A)."""
+    need_ref(orc)
+    A = G.random_csr(90, 70, 0.08, seed=seed, values=True)
+    B = G.random_csr(70, 110, 0.08, seed=seed + 10, values=True)
+    M = G.random_csr(90, 110, 0.1, seed=seed + 20)
+    for a, b, m in ((A, B, M), (M, G.random_csr(110, 90, 0.05, seed=seed), G.random_csr(90, 90, 0.0, seed=1))):
+        want = orc.ref_mxmm_cmask(a, b, m)
+        got = orc.mxmm_cmask(a, b, m)
+        for w, g in zip(want, got):
+            np.testing.assert_array_equal(w, g)
+    S = G.random_csr(120, 120, 0.05, seed=seed)
+    for w, g in zip(orc.ref_mxmm_cmask(S, S, S, parallel=False), orc.mxmm_cmask(S, S, S)):
+        np.testing.assert_array_equal(w, g)
