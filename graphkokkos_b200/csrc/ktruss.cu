@@ -77,22 +77,32 @@ __global__ void k_copy_back(int64_t m, const int64_t *nrp, const int32_t *ncol, 
 // ends a B row past the mask's last column), which roughly halves the streamed
 // entries.  The values are the same integers, so the truss is unchanged.
 
-// Whether every entry (i, j) has its mirror (j, i): warp per row, a binary
-// search in row j per entry.
-__global__ void k_sym_check(int64_t m, const int64_t *rp, const int32_t *col, int *asym) {
+// Row index of every entry (warp per row, coalesced stores).  The per-entry
+// kernels below then spread their work over entries, not rows: with a warp per
+// row, a hub row of 10^5 entries is one warp's serial loop of binary searches
+// and sets the kernel's duration.
+__global__ void k_row_of(int64_t m, const int64_t *rp, int32_t *row) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
-        for (int64_t p = rp[i] + lane; p < rp[i + 1]; p += 32) {
-            const int j = col[p];
-            int64_t lo = rp[j], hi = rp[j + 1];
-            while (lo < hi) {
-                const int64_t md = (lo + hi) >> 1;
-                if (col[md] < i) lo = md + 1;
-                else hi = md;
-            }
-            if (lo == rp[j + 1] || col[lo] != i) atomicExch(asym, 1);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps)
+        for (int64_t p = rp[i] + lane; p < rp[i + 1]; p += 32) row[p] = static_cast<int32_t>(i);
+}
+
+// Whether every entry (i, j) has its mirror (j, i): a thread per entry, a
+// binary search in row j.
+__global__ void k_sym_check(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *row, int *asym) {
+    const int64_t nnz = rp[m];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += stride) {
+        const int i = row[p], j = col[p];
+        int64_t lo = rp[j], hi = rp[j + 1];
+        const int64_t end = hi;
+        while (lo < hi) {
+            const int64_t md = (lo + hi) >> 1;
+            if (col[md] < i) lo = md + 1;
+            else hi = md;
         }
+        if (lo == end || col[lo] != i) atomicExch(asym, 1);
     }
 }
 
@@ -110,42 +120,42 @@ __global__ void k_lower_len(int64_t m, const int64_t *rp, const int32_t *col, in
     }
 }
 
-__global__ void k_lower_fill(int64_t m, const int64_t *rp, const int32_t *col, const int64_t *lrp, int32_t *lcol) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
-        const int64_t n = lrp[i + 1] - lrp[i];
-        for (int64_t k = lane; k < n; k += 32) lcol[lrp[i] + k] = col[rp[i] + k];
+// Lower-triangle columns, a thread per entry of C (balanced over entries).
+__global__ void k_lower_fill(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *row,
+                             const int64_t *lrp, int32_t *lcol) {
+    const int64_t nnz = rp[m];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += stride) {
+        const int i = row[p], j = col[p];
+        const int64_t off = p - rp[i];  // below llen[i] for every j < i of a sorted row
+        if (j < i && off < lrp[i + 1] - lrp[i]) lcol[lrp[i] + off] = j;
     }
 }
 
-// keep[p] for every entry of C from the lower supports: a lower entry reads
-// its own position in L, an upper entry (i, j) the position of i in L's row j.
-__global__ void k_keep_sym(int64_t m, int64_t cap, const int64_t *rp, const int32_t *col, const int64_t *lrp,
-                           const int32_t *lcol, const int32_t *sup, int thresh, int32_t *keep) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += warps) {
-        const int64_t e0 = rp[i], e1 = rp[i + 1];
-        for (int64_t p = e0 + lane; p < e1; p += 32) {
-            const int j = col[p];
-            int64_t q;
-            if (j < i) {
-                q = lrp[i] + (p - e0);
-            } else {
-                int64_t lo = lrp[j], hi = lrp[j + 1];
-                while (lo < hi) {
-                    const int64_t md = (lo + hi) >> 1;
-                    if (lcol[md] < i) lo = md + 1;
-                    else hi = md;
-                }
-                q = (lo < lrp[j + 1] && lcol[lo] == i) ? lo : -1;
-            }
-            keep[p] = (q >= 0 && sup[q] >= thresh) ? 1 : 0;
-        }
-    }
+// keep[p] for every entry of C from the lower supports, a thread per entry: a
+// lower entry reads its own position in L, an upper entry (i, j) the position
+// of i in L's row j (binary search).
+__global__ void k_keep_sym(int64_t m, int64_t cap, const int64_t *rp, const int32_t *col, const int32_t *row,
+                           const int64_t *lrp, const int32_t *lcol, const int32_t *sup, int thresh, int32_t *keep) {
     const int64_t nnz = rp[m];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += stride) {
+        const int i = row[p], j = col[p];
+        int64_t q;
+        if (j < i) {
+            q = lrp[i] + (p - rp[i]);
+        } else {
+            int64_t lo = lrp[j], hi = lrp[j + 1];
+            const int64_t end = hi;
+            while (lo < hi) {
+                const int64_t md = (lo + hi) >> 1;
+                if (lcol[md] < i) lo = md + 1;
+                else hi = md;
+            }
+            q = (lo < end && lcol[lo] == i) ? lo : -1;
+        }
+        keep[p] = (q >= 0 && sup[q] >= thresh) ? 1 : 0;
+    }
     for (int64_t p = nnz + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p <= cap; p += stride) keep[p] = 0;
 }
 
@@ -164,6 +174,7 @@ struct KtBuffers {
     bool sym;                  // symmetric input: support on the lower triangle
     int64_t *llen, *lrp;       // lower-triangle lengths (m + 1) and row pointers (m + 1)
     int32_t *lcol;             // lower-triangle columns
+    int32_t *row;              // row index of every entry of the current matrix
 };
 
 // One pass: support S<C> = C·C, flags, scan, compaction, pass end, copy back.
@@ -180,16 +191,18 @@ static int ktruss_pass(const KtBuffers &b, cudaStream_t s, cudaGraphConditionalH
     rq.stream = s;
     size_t scan_bytes = b.scan_bytes;
     if (b.sym) {
+        k_row_of<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.row);
         k_lower_len<<<sms * 4, 256, 0, s>>>(b.m, b.rp, b.col, b.llen);
         GK_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, scan_bytes, b.llen, b.lrp, b.m + 1, s));
-        k_lower_fill<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.col, b.lrp, b.lcol);
+        k_lower_fill<<<sms * 8, 256, 0, s>>>(b.m, b.rp, b.col, b.row, b.lrp, b.lcol);
         rq.M = DevCsr{b.m, b.m, b.cap, b.lrp, b.lcol, nullptr};
         GK_CHECK(run_spgemm(rq, pass));
-        k_keep_sym<<<sms * 8, 256, 0, s>>>(b.m, b.cap, b.rp, b.col, b.lrp, b.lcol, b.sup, b.k - 2, b.keep);
-        note_launches(3);
+        k_keep_sym<<<sms * 8, 256, 0, s>>>(b.m, b.cap, b.rp, b.col, b.row, b.lrp, b.lcol, b.sup, b.k - 2, b.keep);
+        note_launches(4);
     } else {
         GK_CHECK(run_spgemm(rq, pass));
         k_keep_flags<<<sms * 8, 256, 0, s>>>(b.sup, b.rp, b.m, b.cap, b.k - 2, b.keep);
+        note_launches(1);
     }
     scan_bytes = b.scan_bytes;
     GK_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, scan_bytes, b.keep, b.pos, b.cap + 1, s));
@@ -276,13 +289,15 @@ int ktruss_device(int64_t m, int64_t nnz0, int64_t *rp_a, int32_t *col_a, int k,
     GK_CHECK(scr.alloc(&b.llen, m + 1));
     GK_CHECK(scr.alloc(&b.lrp, m + 1));
     GK_CHECK(scr.alloc(&b.lcol, nnz0));
+    GK_CHECK(scr.alloc(&b.row, nnz0));
     GK_CUDA(cudaMemsetAsync(b.llen + m, 0, sizeof(int64_t), s));
     {
         int *asym;
         GK_CHECK(scr.alloc(&asym, 1));
         GK_CUDA(cudaMemsetAsync(asym, 0, sizeof(int), s));
-        k_sym_check<<<ctx().num_sms * 8, 256, 0, s>>>(m, rp_a, col_a, asym);
-        note_launches(1);
+        k_row_of<<<ctx().num_sms * 8, 256, 0, s>>>(m, rp_a, b.row);
+        k_sym_check<<<ctx().num_sms * 8, 256, 0, s>>>(m, rp_a, col_a, b.row, asym);
+        note_launches(2);
         int h = 1;
         GK_CUDA(cudaMemcpyAsync(&h, asym, sizeof(int), cudaMemcpyDeviceToHost, s));
         GK_CUDA(cudaStreamSynchronize(s));

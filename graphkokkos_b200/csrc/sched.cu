@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -69,10 +70,20 @@ __host__ __device__ inline int forced_variant(int bin, const BinStats &b, int ac
 
 // The learned choice replaces the plain one only where the model predicts it
 // at least this much faster (log2 of 1.1): small predicted gains are within the
-// model's error and are not worth a change of kernel.
+// model's error and are not worth a change of kernel.  GK_LEARNED_MARGIN (a
+// log2 ratio) overrides it, for tuning runs.
 constexpr float LEARNED_MARGIN = 0.1375f;
 
-__device__ inline int mlp_variant(const float *w, const float *f_raw, int bin, int plain) {
+static float learned_margin() {
+    static const float m = [] {
+        const char *e = getenv("GK_LEARNED_MARGIN");
+        const float v = e ? static_cast<float>(atof(e)) : LEARNED_MARGIN;
+        return std::isfinite(v) && v >= 0.f ? v : LEARNED_MARGIN;
+    }();
+    return m;
+}
+
+__device__ inline int mlp_variant(const float *w, const float *f_raw, int bin, int plain, float margin) {
     const float *W1 = w;
     const float *b1 = W1 + MLP_H * NFEAT;
     const float *W2 = b1 + MLP_H;
@@ -105,10 +116,11 @@ __device__ inline int mlp_variant(const float *w, const float *f_raw, int bin, i
             best = v;
         }
     }
-    return plain_s - best_s >= LEARNED_MARGIN ? best : plain;
+    return plain_s - best_s >= margin ? best : plain;
 }
 
-__global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int accum, int epi, bool values) {
+__global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int accum, int epi, bool values,
+                         float margin) {
     // the weights are read by every bin's thread: stage them in shared memory
     // (broadcast reads) instead of chains of dependent global loads
     __shared__ float sw[MLP_SIZE];
@@ -129,7 +141,7 @@ __global__ void k_choose(const BinStats *bins, int *var_of_bin, int mode, int ac
     else if (mode == GK_SCHED_LEARNED) {
         float f[NFEAT];
         bin_features(st, epi, values, f);
-        v = mlp_variant(sw, f, b, plain_variant(b, st));
+        v = mlp_variant(sw, f, b, plain_variant(b, st), margin);
     } else v = plain_variant(b, st);
     var_of_bin[b] = v;
 }
@@ -159,7 +171,7 @@ int sched_prepare(int sched, int force_accum) {
 int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_accum, int epi, bool values,
                  cudaStream_t s) {
     GK_CHECK(sched_prepare(sched, force_accum));
-    k_choose<<<1, NBINS, 0, s>>>(bins, var_of_bin, sched, force_accum, epi, values);
+    k_choose<<<1, NBINS, 0, s>>>(bins, var_of_bin, sched, force_accum, epi, values, learned_margin());
     GK_CUDA(cudaGetLastError());
     return GK_OK;
 }

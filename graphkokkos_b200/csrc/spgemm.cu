@@ -63,7 +63,29 @@ __global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
         const int64_t a0 = A.rp[r], a1 = A.rp[r + 1];
         long long w = 0;
         int mb = 0;
-        for (int64_t t = a0 + lane; t < a1; t += 32) {
+        int64_t t = a0 + lane;
+        // eight independent column / row-pointer load pairs in flight per lane:
+        // a hub row (10^5 entries) is one warp's loop, and its length in
+        // dependent load latencies bounds the kernel
+        constexpr int U = 8;
+        for (; t + 32 * (U - 1) < a1; t += 32 * U) {
+            int k[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) k[u] = __ldg(A.col + t + 32 * u);
+            int64_t b0[U], b1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                b0[u] = __ldg(B.rp + k[u]);
+                b1[u] = __ldg(B.rp + k[u] + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int len = static_cast<int>(b1[u] - b0[u]);
+                w += len;
+                mb = max(mb, len);
+            }
+        }
+        for (; t < a1; t += 32) {
             const int k = __ldg(A.col + t);
             const int len = static_cast<int>(__ldg(B.rp + k + 1) - __ldg(B.rp + k));
             w += len;
