@@ -4,6 +4,8 @@
 // the caller's stream and returns outputs to host or device memory.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "gk_common.cuh"
@@ -61,13 +63,16 @@ struct GraphSlot {
     int64_t m, nnz, vbase, ebase;
 };
 
-__global__ void k_concat_graphs(const GraphSlot *slots, int64_t *rp_out, int32_t *col_out, int32_t *key_out) {
+// Graph key_base + blockIdx.x of the batch into the combined matrix (slots
+// points at that graph's slot for blockIdx.x == 0).
+__global__ void k_concat_graphs(const GraphSlot *slots, int key_base, int64_t *rp_out, int32_t *col_out,
+                                int32_t *key_out) {
     const GraphSlot g = slots[blockIdx.x];
     const int64_t stride = (int64_t)gridDim.y * blockDim.x;
     const int64_t start = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
     for (int64_t i = start; i < g.m; i += stride) {
         rp_out[g.vbase + i] = g.rp[i] - g.rp[0] + g.ebase;
-        key_out[g.vbase + i] = static_cast<int32_t>(blockIdx.x);
+        key_out[g.vbase + i] = key_base + static_cast<int32_t>(blockIdx.x);
     }
     const int64_t off = g.rp[0];
     for (int64_t j = start; j < g.nnz; j += stride)
@@ -382,22 +387,20 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
     GK_CHECK(scr.alloc(&rp, vtot + 1));
     GK_CHECK(scr.alloc(&col, etot > 0 ? etot : 1));
     GK_CHECK(scr.alloc(&key, vtot > 0 ? vtot : 1));
+    unsigned long long *d;
+    GK_CHECK(scr.alloc(&d, ngraphs));
+    GK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * ngraphs, s));
+    int64_t *rp_raw = nullptr;
     if (any_host) {
-        // stage every graph raw into the combined buffers, then offset in place
-        int64_t *rp_raw;
+        // host graphs are staged raw into the combined buffers (columns at their
+        // final positions, offset in place by k_concat_graphs)
         GK_CHECK(scr.alloc(&rp_raw, vtot + ngraphs));
         int64_t roff = 0;
         for (int g = 0; g < ngraphs; ++g) {
-            GK_CUDA(cudaMemcpyAsync(rp_raw + roff, graphs[g].rowptr, sizeof(int64_t) * (graphs[g].m + 1),
-                                    cudaMemcpyDefault, s));
-            if (graphs[g].nnz)
-                GK_CUDA(cudaMemcpyAsync(col + slots[g].ebase, graphs[g].col, sizeof(int32_t) * graphs[g].nnz,
-                                        cudaMemcpyDefault, s));
             slots[g].rp = rp_raw + roff;
             slots[g].col = col + slots[g].ebase;
             roff += graphs[g].m + 1;
         }
-        // col is already in place: rewrite it in place with the vertex offset
     } else {
         for (int g = 0; g < ngraphs; ++g) {
             slots[g].rp = graphs[g].rowptr;
@@ -407,29 +410,102 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
     GraphSlot *dslots;
     GK_CHECK(scr.alloc(&dslots, ngraphs));
     GK_CUDA(cudaMemcpyAsync(dslots, slots.data(), sizeof(GraphSlot) * ngraphs, cudaMemcpyHostToDevice, s));
+
+    // Groups of consecutive graphs.  With host inputs the copies of group q+1
+    // run on a side stream while group q is counted (the graphs are
+    // independent, so a group needs only its own rows); device inputs form one
+    // group.  A group holds about etot/8 entries, at least GK_BATCH_STAGE_MIN
+    // (default 2^24, whose copy takes ~1 ms).  All copies are queued at once,
+    // so they run back to back while the counts follow them group by group.
+    // (Groups that double in size, which expose only a small first copy, were
+    // slower on the uneven 4,096-graph batch: its compute-light Erdos-Renyi
+    // half comes first and cannot hide the copies of the large groups.)
+    std::vector<int> gstart{0};
     if (any_host) {
-        // the raw col copies sit at their final positions; k_concat_graphs reads
-        // them with offset rp[0] == 0 relative to the slot's own col pointer
+        int64_t min_entries = int64_t(1) << 24;
+        if (const char *e = getenv("GK_BATCH_STAGE_MIN")) min_entries = std::max<int64_t>(1, atoll(e));
+        const int64_t target = std::max<int64_t>(etot / 8, min_entries);
+        int64_t acc = 0;
+        for (int g = 0; g + 1 < ngraphs; ++g) {
+            acc += graphs[g].nnz;
+            if (acc >= target) {
+                gstart.push_back(g + 1);
+                acc = 0;
+            }
+        }
     }
-    dim3 grid(ngraphs, 8);
-    k_concat_graphs<<<grid, 256, 0, s>>>(dslots, rp, col, key);
-    note_launches(1);
-    GK_CUDA(cudaGetLastError());
-    k_set_last<<<1, 1, 0, s>>>(rp, vtot, etot);
-    note_launches(1);
-    GK_CUDA(cudaGetLastError());
-    unsigned long long *d;
-    GK_CHECK(scr.alloc(&d, ngraphs));
-    GK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * ngraphs, s));
-    DevCsr dc{vtot, vtot, etot, rp, col, nullptr};
-    SpgemmRequest rq;
-    rq.A = rq.B = rq.M = dc;
-    rq.epi = EPI_KEYED;
-    rq.row_key = key;
-    rq.sums = d;
-    rq.sched = sched;
-    rq.stream = s;
-    GK_CHECK(run_spgemm(rq, scr));
+    gstart.push_back(ngraphs);
+    const int ngroups = static_cast<int>(gstart.size()) - 1;
+
+    // side stream and events, released on every return path; the caller's
+    // stream first waits for the side stream, so that the scratch (freed in
+    // order on the caller's stream) outlives every copy into it
+    struct Pipe {
+        cudaStream_t s, cs = nullptr;
+        std::vector<cudaEvent_t> ev;
+        explicit Pipe(cudaStream_t s_) : s(s_) {}
+        ~Pipe() {
+            if (cs) {
+                cudaEvent_t done;
+                if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+                    cudaEventRecord(done, cs);
+                    cudaStreamWaitEvent(s, done, 0);
+                    cudaEventDestroy(done);
+                } else {
+                    cudaStreamSynchronize(cs);
+                }
+            }
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+            if (cs) cudaStreamDestroy(cs);
+        }
+    } pipe(s);
+    cudaStream_t cs = s;
+    if (any_host && ngroups > 1) {
+        GK_CUDA(cudaStreamCreateWithFlags(&pipe.cs, cudaStreamNonBlocking));
+        cs = pipe.cs;
+        pipe.ev.resize(ngroups + 1, nullptr);
+        for (auto &e : pipe.ev) GK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        GK_CUDA(cudaEventRecord(pipe.ev[ngroups], s));  // buffers allocated, sums zeroed
+        GK_CUDA(cudaStreamWaitEvent(cs, pipe.ev[ngroups], 0));
+    }
+    for (int q = 0; q < ngroups; ++q) {
+        const int g0 = gstart[q], g1 = gstart[q + 1];
+        if (any_host) {
+            for (int g = g0; g < g1; ++g) {
+                GK_CUDA(cudaMemcpyAsync(const_cast<int64_t *>(slots[g].rp), graphs[g].rowptr,
+                                        sizeof(int64_t) * (graphs[g].m + 1), cudaMemcpyDefault, cs));
+                if (graphs[g].nnz)
+                    GK_CUDA(cudaMemcpyAsync(col + slots[g].ebase, graphs[g].col, sizeof(int32_t) * graphs[g].nnz,
+                                            cudaMemcpyDefault, cs));
+            }
+            if (cs != s) {
+                GK_CUDA(cudaEventRecord(pipe.ev[q], cs));
+                GK_CUDA(cudaStreamWaitEvent(s, pipe.ev[q], 0));
+            }
+        }
+        const int64_t v0 = slots[g0].vbase, e0 = slots[g0].ebase;
+        const int64_t v1 = g1 < ngraphs ? slots[g1].vbase : vtot, e1 = g1 < ngraphs ? slots[g1].ebase : etot;
+        dim3 grid(g1 - g0, 8);
+        k_concat_graphs<<<grid, 256, 0, s>>>(dslots + g0, g0, rp, col, key);
+        k_set_last<<<1, 1, 0, s>>>(rp, v1, e1);  // the group's end (the next group writes the same value)
+        note_launches(2);
+        GK_CUDA(cudaGetLastError());
+        // rows [v0, v1) against the whole combined matrix: their columns lie in
+        // [v0, v1), so only this group's B rows are read
+        DevCsr rows{v1 - v0, vtot, e1 - e0, rp + v0, col, nullptr};
+        DevCsr all{vtot, vtot, etot, rp, col, nullptr};
+        SpgemmRequest rq;
+        rq.A = rq.M = rows;
+        rq.B = all;
+        rq.epi = EPI_KEYED;
+        rq.row_key = key + v0;
+        rq.sums = d;
+        rq.sched = sched;
+        rq.stream = s;
+        Scratch gs(s);  // the group's plan, freed in stream order before the next group's
+        GK_CHECK(run_spgemm(rq, gs));
+    }
     return deliver(counts, d, sizeof(uint64_t) * ngraphs, s);
 }
 

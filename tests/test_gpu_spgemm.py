@@ -99,6 +99,31 @@ def test_tc_batched(gk, orc, cuda):
     np.testing.assert_array_equal(got_dev, want)
 
 
+@pytest.mark.parametrize("sched", ["plain", "learned"])
+def test_tc_batched_host_groups(gk, orc, cuda, monkeypatch, sched):
+    """Host graphs are copied and counted in groups (the copies of the next
+    group overlap the count of this one); a small group size forces many groups,
+    some of them holding only edgeless graphs."""
+    if sched == "learned":
+        from graphkokkos_b200 import sched as S
+        S.load_model()
+    graphs = []
+    for i in range(30):
+        if i in (3, 4, 5, 17):
+            graphs.append(gk.lower_host(G.empty(7 + i)))
+        elif i % 3 == 0:
+            graphs.append(gk.lower_host(gk.gen_er(300 + 41 * i, 2500 + 200 * i, seed=500 + i)))
+        else:
+            graphs.append(gk.lower_host(gk.gen_rmat(5 + i % 6, 16, seed=500 + i)))
+    want = np.array([orc.tc_lower(L) for L in graphs], dtype=np.uint64)
+    for stage_min in ("1", "3000", "40000"):
+        monkeypatch.setenv("GK_BATCH_STAGE_MIN", stage_min)
+        np.testing.assert_array_equal(gk.tc_count_batched(graphs, sched=sched), want)
+    # host and device graphs mixed in one batch
+    mixed = [dev(L) if i % 4 == 1 else L for i, L in enumerate(graphs)]
+    np.testing.assert_array_equal(gk.tc_count_batched(mixed, sched=sched), want)
+
+
 # ---------------------------------------------------------------------------
 # general masked SpGEMM with values (plus-times)
 # ---------------------------------------------------------------------------
