@@ -43,7 +43,7 @@ static int check_square_pattern(const gk_csr *L, const char *name) {
 static int tc_common(const gk_csr *L, int epi, unsigned long long *dev_sums, int sched, cudaStream_t s,
                      Scratch &scr, int force_variant = -1) {
     DevCsr d;
-    GK_CHECK(stage_csr(L, &d, scr, s));
+    GK_CHECK(stage_csr(L, &d, scr, s, nullptr, CSR_SORTED, "L"));
     d.val = nullptr;  // plus-pair: an adjacency pattern
     SpgemmRequest rq;
     rq.A = rq.B = rq.M = d;
@@ -64,19 +64,35 @@ struct GraphSlot {
 };
 
 // Graph key_base + blockIdx.x of the batch into the combined matrix (slots
-// points at that graph's slot for blockIdx.x == 0).
+// points at that graph's slot for blockIdx.x == 0).  Row pointers must run
+// from 0 to nnz (spMtx's invariant, matrix.h:33-43); a pointer outside [0, nnz]
+// is clamped into the graph's own entry range, so the combined matrix never
+// points outside its buffers; a column outside [0, m) is replaced by 0 (the
+// graph's first vertex).  Each defect is flagged in *bad for the check that
+// follows.
 __global__ void k_concat_graphs(const GraphSlot *slots, int key_base, int64_t *rp_out, int32_t *col_out,
-                                int32_t *key_out) {
+                                int32_t *key_out, unsigned int *bad) {
     const GraphSlot g = slots[blockIdx.x];
     const int64_t stride = (int64_t)gridDim.y * blockDim.x;
     const int64_t start = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+    if (start == 0 && (g.rp[0] != 0 || g.rp[g.m] != g.nnz)) atomicOr(bad, CSR_BAD_ENDS);
     for (int64_t i = start; i < g.m; i += stride) {
-        rp_out[g.vbase + i] = g.rp[i] - g.rp[0] + g.ebase;
+        int64_t p = g.rp[i];
+        if (p < 0 || p > g.nnz) {
+            atomicOr(bad, CSR_BAD_ROWPTR);
+            p = p < 0 ? 0 : g.nnz;
+        }
+        rp_out[g.vbase + i] = p + g.ebase;
         key_out[g.vbase + i] = key_base + static_cast<int32_t>(blockIdx.x);
     }
-    const int64_t off = g.rp[0];
-    for (int64_t j = start; j < g.nnz; j += stride)
-        col_out[g.ebase + j] = g.col[off + j] + static_cast<int32_t>(g.vbase);
+    for (int64_t j = start; j < g.nnz; j += stride) {
+        int32_t x = g.col[j];
+        if (x < 0 || x >= g.m) {  // outside the graph's own vertices
+            atomicOr(bad, CSR_BAD_COL);
+            x = 0;
+        }
+        col_out[g.ebase + j] = x + static_cast<int32_t>(g.vbase);
+    }
 }
 
 __global__ void k_set_last(int64_t *rp, int64_t idx, int64_t value) { rp[idx] = value; }
@@ -211,9 +227,9 @@ int gk_mxmm_masked(const gk_csr *A, const gk_csr *B, const gk_csr *M, int32_t *C
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     SpgemmRequest rq;
-    GK_CHECK(stage_csr(A, &rq.A, scr, s));
-    GK_CHECK(stage_csr(B, &rq.B, scr, s));
-    GK_CHECK(stage_csr(M, &rq.M, scr, s));
+    GK_CHECK(stage_csr(A, &rq.A, scr, s, nullptr, CSR_STRUCTURE, "A"));
+    GK_CHECK(stage_csr(B, &rq.B, scr, s, nullptr, CSR_SORTED, "B"));
+    GK_CHECK(stage_csr(M, &rq.M, scr, s, nullptr, CSR_SORTED, "M"));
     rq.M.val = nullptr;
     rq.epi = EPI_WRITE;
     rq.use_values = semiring == GK_PLUS_TIMES;
@@ -266,9 +282,9 @@ int gk_mxmm_masked_variant(const gk_csr *A, const gk_csr *B, const gk_csr *M, in
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     SpgemmRequest rq;
-    GK_CHECK(stage_csr(A, &rq.A, scr, s));
-    GK_CHECK(stage_csr(B, &rq.B, scr, s));
-    GK_CHECK(stage_csr(M, &rq.M, scr, s));
+    GK_CHECK(stage_csr(A, &rq.A, scr, s, nullptr, CSR_STRUCTURE, "A"));
+    GK_CHECK(stage_csr(B, &rq.B, scr, s, nullptr, CSR_SORTED, "B"));
+    GK_CHECK(stage_csr(M, &rq.M, scr, s, nullptr, CSR_SORTED, "M"));
     rq.M.val = nullptr;
     rq.epi = EPI_WRITE;
     rq.use_values = semiring == GK_PLUS_TIMES;
@@ -303,7 +319,7 @@ int gk_tc_vertex(const gk_csr *A, int32_t *counts, int sched, void *stream) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr d;
-    GK_CHECK(stage_csr(A, &d, scr, s));
+    GK_CHECK(stage_csr(A, &d, scr, s, nullptr, CSR_SORTED, "A"));
     d.val = nullptr;
     unsigned long long *sums;
     int32_t *out;
@@ -329,7 +345,7 @@ int gk_tc_count_lu(const gk_csr *A, uint64_t *count, int sched, void *stream) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr d;
-    GK_CHECK(stage_csr(A, &d, scr, s));
+    GK_CHECK(stage_csr(A, &d, scr, s, nullptr, CSR_SORTED, "A"));
     d.val = nullptr;
     const int64_t m = A->m;
     int64_t *lrp, *urp;
@@ -410,6 +426,16 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
     GraphSlot *dslots;
     GK_CHECK(scr.alloc(&dslots, ngraphs));
     GK_CUDA(cudaMemcpyAsync(dslots, slots.data(), sizeof(GraphSlot) * ngraphs, cudaMemcpyHostToDevice, s));
+    // per-graph entry ranges for the content check, and its flags
+    std::vector<int64_t> ranges(static_cast<size_t>(ngraphs) + 1);
+    for (int g = 0; g < ngraphs; ++g) ranges[g] = slots[g].ebase;
+    ranges[ngraphs] = etot;
+    int64_t *dranges;
+    unsigned int *bad;
+    GK_CHECK(scr.alloc(&dranges, ranges.size()));
+    GK_CHECK(scr.alloc(&bad, 1));
+    GK_CUDA(cudaMemcpyAsync(dranges, ranges.data(), sizeof(int64_t) * ranges.size(), cudaMemcpyHostToDevice, s));
+    GK_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned int), s));
 
     // Groups of consecutive graphs.  With host inputs the copies of group q+1
     // run on a side stream while group q is counted (the graphs are
@@ -487,7 +513,7 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
         const int64_t v0 = slots[g0].vbase, e0 = slots[g0].ebase;
         const int64_t v1 = g1 < ngraphs ? slots[g1].vbase : vtot, e1 = g1 < ngraphs ? slots[g1].ebase : etot;
         dim3 grid(g1 - g0, 8);
-        k_concat_graphs<<<grid, 256, 0, s>>>(dslots + g0, g0, rp, col, key);
+        k_concat_graphs<<<grid, 256, 0, s>>>(dslots + g0, g0, rp, col, key, bad);
         k_set_last<<<1, 1, 0, s>>>(rp, v1, e1);  // the group's end (the next group writes the same value)
         note_launches(2);
         GK_CUDA(cudaGetLastError());
@@ -504,6 +530,7 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
         rq.sched = sched;
         rq.stream = s;
         Scratch gs(s);  // the group's plan, freed in stream order before the next group's
+        GK_CHECK(check_csr_batch(rows, e0, v0, key, dranges, bad, CSR_SORTED, "graphs", s, gs));
         GK_CHECK(run_spgemm(rq, gs));
     }
     return deliver(counts, d, sizeof(uint64_t) * ngraphs, s);
@@ -515,7 +542,7 @@ int gk_extract_lower(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr d;
-    GK_CHECK(stage_csr(A, &d, scr, s));
+    GK_CHECK(stage_csr(A, &d, scr, s, nullptr, CSR_SORTED, "A"));
     const bool host_out = !is_device_pointer(out_rowptr);
     int64_t *orp = out_rowptr;
     int32_t *ocol = out_col;
@@ -541,7 +568,7 @@ int gk_transpose(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int32_t
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr d;
-    GK_CHECK(stage_csr(A, &d, scr, s));
+    GK_CHECK(stage_csr(A, &d, scr, s, nullptr, CSR_STRUCTURE, "A"));
     const bool host_out = !is_device_pointer(out_rowptr);
     int64_t *orp = out_rowptr;
     int32_t *ocol = out_col, *oval = out_val;

@@ -1158,7 +1158,7 @@ static int bc_entry(const gk_csr *A, const int32_t *sources, int nsources, doubl
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr d;
-    GK_CHECK(stage_csr(A, &d, scr, s));
+    GK_CHECK(stage_csr(A, &d, scr, s, nullptr, CSR_STRUCTURE, "A"));
     // sources: validate on the host
     std::vector<int32_t> hs(nsources > 0 ? nsources : 1);
     if (nsources > 0) {

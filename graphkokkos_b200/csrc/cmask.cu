@@ -131,9 +131,9 @@ extern "C" int gk_mxmm_cmask(const gk_csr *A, const gk_csr *B, const gk_csr *M, 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scr(s);
     DevCsr a, b, mk;
-    GK_CHECK(stage_csr(A, &a, scr, s));
-    GK_CHECK(stage_csr(B, &b, scr, s));
-    GK_CHECK(stage_csr(M, &mk, scr, s));
+    GK_CHECK(stage_csr(A, &a, scr, s, nullptr, CSR_STRUCTURE, "A"));
+    GK_CHECK(stage_csr(B, &b, scr, s, nullptr, CSR_STRUCTURE, "B"));
+    GK_CHECK(stage_csr(M, &mk, scr, s, nullptr, CSR_SORTED, "M"));
     const bool values = semiring == GK_PLUS_TIMES;
     const int64_t m = A->m;
     const bool fill = C_col != nullptr;

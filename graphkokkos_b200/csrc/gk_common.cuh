@@ -78,9 +78,32 @@ private:
     size_t arena_bytes_ = 0, arena_used_ = 0;
 };
 
+// What check_csr verifies beyond the row pointers and the column range.
+enum CsrCheck { CSR_STRUCTURE = 1, CSR_SORTED = 2 };
+
+// Content check of a CSR already in device memory, one warp per row: row
+// pointers from 0 to nnz and non-decreasing, columns in [0, n), and with
+// CSR_SORTED columns strictly increasing within each row (sorted, no
+// duplicates).  Returns GK_ERR_INVALID_CSR with the first bad row.  It reads
+// the result on the host (one synchronisation); inside a stream capture, or
+// with GK_CHECK_CSR=0 in the environment, it is skipped.
+int check_csr(const DevCsr &d, int level, const char *name, cudaStream_t s, Scratch &scr);
+// The same for rows [row_base, row_base + m) of a block-diagonal batch whose
+// row pointers run from ebase to ebase + nnz: row r belongs to graph
+// key[row_base + r] (indices into the combined matrix), whose entries must lie
+// in [estart[g], estart[g+1]].  pre_flags (device, may be null) holds CsrBad
+// flags found while the batch was assembled (a column outside its graph's
+// vertex range, a graph's row pointers not from 0 to nnz); they are reported
+// like the check's own.
+enum CsrBad : unsigned int { CSR_BAD_ENDS = 1, CSR_BAD_ROWPTR = 2, CSR_BAD_COL = 4, CSR_BAD_ORDER = 8 };
+int check_csr_batch(const DevCsr &d, int64_t ebase, int64_t row_base, const int32_t *key, const int64_t *estart,
+                    const unsigned int *pre_flags, int level, const char *name, cudaStream_t s, Scratch &scr);
+
 // Host-or-device staging of a CSR: if the arrays are host memory they are
-// copied to HBM on the stream (into scratch), otherwise used in place.
-int stage_csr(const gk_csr *in, DevCsr *out, Scratch &scr, cudaStream_t s, int64_t *h2d_bytes = nullptr);
+// copied to HBM on the stream (into scratch), otherwise used in place.  With
+// check > 0 the staged matrix then goes through check_csr at that level.
+int stage_csr(const gk_csr *in, DevCsr *out, Scratch &scr, cudaStream_t s, int64_t *h2d_bytes = nullptr,
+              int check = CSR_SORTED, const char *name = "matrix");
 bool is_device_pointer(const void *p);
 int validate_csr_shape(const gk_csr *c, const char *name);
 

@@ -362,6 +362,7 @@ extern "C" int gk_ktruss(gk_csr_mut *inout, int k, int *iters, int sched, void *
     GK_CHECK(scr.alloc(&col, nnz0 > 0 ? nnz0 : 1));
     GK_CUDA(cudaMemcpyAsync(rp, inout->rowptr, sizeof(int64_t) * (m + 1), cudaMemcpyDefault, s));
     if (nnz0) GK_CUDA(cudaMemcpyAsync(col, inout->col, sizeof(int32_t) * nnz0, cudaMemcpyDefault, s));
+    GK_CHECK(check_csr(DevCsr{m, m, nnz0, rp, col, nullptr}, CSR_SORTED, "graph", s, scr));
     int64_t nnz = 0;
     int64_t *rp_res;
     int32_t *col_res;

@@ -19,6 +19,9 @@
 //  * The array's device address is fetched with cudaGetSymbolAddress the first
 //    time the entry point is called on a device (with that device current);
 //    that first call should therefore come before any stream capture.
+//  * L goes through the same content check as every entry point (row
+//    pointers, column range, sorted rows), which synchronises the stream once;
+//    GK_CHECK_CSR=0 skips it for trusted input.
 //  * All calls share the array and it keeps the last call's contents; what
 //    must start at zero is cleared by each call.  Calls whose work overlaps on
 //    the GPU (other host threads, or other streams without ordering between
@@ -77,6 +80,7 @@ extern "C" int gk_tc_count_noalloc(const gk_csr *L, uint64_t *count, int sched, 
     GK_CHECK(scr.alloc(&d, 1));
     GK_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
     DevCsr dl{L->m, L->n, L->nnz, L->rowptr, L->col, nullptr};
+    GK_CHECK(check_csr(dl, CSR_SORTED, "L", s, scr));
     SpgemmRequest rq;
     rq.A = rq.B = rq.M = dl;
     rq.epi = EPI_SUM;

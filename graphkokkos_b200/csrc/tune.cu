@@ -24,7 +24,7 @@ static int tune_request(const gk_csr *G, int mode, SpgemmRequest &rq, Scratch &s
     GK_CHECK(validate_csr_shape(G, "G"));
     if (G->m != G->n) return fail(GK_ERR_ARG, "tune: matrix must be square");
     DevCsr d;
-    GK_CHECK(stage_csr(G, &d, scr, s));
+    GK_CHECK(stage_csr(G, &d, scr, s, nullptr, CSR_SORTED, "graph"));
     d.val = nullptr;
     rq.A = rq.B = rq.M = d;
     rq.stream = s;

@@ -21,6 +21,16 @@
  *  - Every entry point returns a gk_status; on failure gk_last_error_string()
  *    describes the error for the calling host thread.  Calls on different
  *    streams may run concurrently.
+ *  - Every matrix argument is checked on the device before any kernel indexes
+ *    through it: row pointers from 0 to nnz and non-decreasing, columns in
+ *    [0, n), and (except A of the masked products, A and B of the
+ *    complement-masked product, and the inputs of gk_transpose and
+ *    gk_bc_batch, whose order does not matter) columns strictly increasing
+ *    within each row.  A violation returns GK_ERR_INVALID_CSR naming the
+ *    matrix, the defect and the first bad row.  The check reads the result on
+ *    the host (one synchronisation of `stream`); it is skipped inside a
+ *    stream capture and when the environment sets GK_CHECK_CSR=0, in which
+ *    case the caller guarantees well-formed input.
  *  - Results are bit-exact with the reference on the same inputs: integer
  *    outputs exactly, FP64 betweenness scores to round-off (the scheduler
  *    changes only the order of FP64 sums).
