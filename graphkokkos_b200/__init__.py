@@ -1,13 +1,15 @@
 """GraphKokkos-B200: masked SpGEMM C<M> = A·B and triangle counting, k-truss
 and batched betweenness centrality on one B200, behind the reference's
 operator surface.  See include/gk_b200.h for the C ABI."""
-from .api import (Csr, bc_batch, extract_lower, gen_er, gen_rmat, ktruss, lower_host, mxmm_cmask, mxmm_masked, read_matrix,
+from .api import (Csr, add_nointersect, bc_batch, dense_ewise_mult_masked, dense_fuse_ewise_mult_add, extract_lower,
+                  gen_er, gen_rmat, ktruss, lower_host, mxmm_cmask, mxmm_masked, mxmm_spd, read_matrix,
                   write_matrix,
                   mxmm_masked_variant, num_variants, tc_count, tc_count_batched, tc_count_device, tc_count_lu,
                   tc_count_variant, tc_row_sums, tc_vertex, transpose)
 from ._lib import GkError, LIB_PATH, load
 
 __all__ = [
-    "Csr", "GkError", "LIB_PATH", "bc_batch", "extract_lower", "gen_er", "gen_rmat", "ktruss", "load",
+    "Csr", "GkError", "LIB_PATH", "add_nointersect", "bc_batch", "dense_ewise_mult_masked",
+    "dense_fuse_ewise_mult_add", "mxmm_spd", "extract_lower", "gen_er", "gen_rmat", "ktruss", "load",
     "lower_host", "mxmm_cmask", "mxmm_masked", "read_matrix", "write_matrix", "mxmm_masked_variant", "num_variants", "tc_count", "tc_count_variant", "tc_count_batched", "tc_count_device", "tc_count_lu", "tc_row_sums", "tc_vertex", "transpose",
 ]

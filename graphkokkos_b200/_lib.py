@@ -86,6 +86,11 @@ SIGNATURES = {
     "gk_tc_vertex": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
     "gk_mxmm_cmask": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 3 + [ctypes.c_int, VP, VP, VP, VP]),
     "gk_tc_count_lu": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP]),
+    "gk_add_nointersect": (ctypes.c_int, [ctypes.POINTER(GkCsr)] * 2 + [VP, VP, VP, VP]),
+    "gk_dense_ewise_mult_masked": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, VP, VP, ctypes.POINTER(GkCsr), VP,
+                                                  VP]),
+    "gk_dense_fuse_ewise_mult_add": (ctypes.c_int, [ctypes.c_int64, VP, VP, VP, VP]),
+    "gk_mxmm_spd": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, VP, ctypes.c_int64, ctypes.POINTER(GkCsr), VP, VP]),
     "gk_tc_count_batched": (ctypes.c_int, [ctypes.POINTER(GkCsr), ctypes.c_int, VP, ctypes.c_int, VP]),
     "gk_ktruss": (ctypes.c_int, [ctypes.POINTER(GkCsrMut), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, VP]),
     "gk_bc_batch": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP, ctypes.c_int, VP]),

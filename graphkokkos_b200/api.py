@@ -190,6 +190,81 @@ def mxmm_cmask(A: Csr, B: Csr, M: Csr, semiring="plus_times", stream=None) -> Cs
     return Csr(A.m, B.n, rp, col[:nnz], val[:nnz], nnz)
 
 
+# ---------------------------------------------------------------------------
+# operators of the reference's alternate BC formulation
+# (include/matrix_la.h:182-328; dense operands are row-major float64)
+# ---------------------------------------------------------------------------
+def _dense(x):
+    """A C-contiguous float64 array (numpy) or tensor (torch, same device)."""
+    if _is_torch(x):
+        import torch
+        return x.to(torch.float64).contiguous()
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def add_nointersect(A: Csr, B: Csr, stream=None) -> Csr:
+    """C = A + B for non-intersecting patterns (add_nointersect,
+    include/matrix_la.h:287-328): each row the merge of A's and B's rows.
+    Returned in the memory space of A; pattern-only operands count as 1."""
+    lib = _lib.load()
+    nnz = A.nnz + B.nnz
+    rp = _empty_like_space(A.rowptr, (A.m + 1,), np.int64)
+    col = _empty_like_space(A.rowptr, (max(nnz, 1),), np.int32)
+    val = _empty_like_space(A.rowptr, (max(nnz, 1),), np.int32)
+    ga, gb = A.as_gk(), B.as_gk()
+    check(lib.gk_add_nointersect(ctypes.byref(ga), ctypes.byref(gb), _ptr(rp), _ptr(col), _ptr(val),
+                                 _stream(stream, A.col, B.col)))
+    return Csr(A.m, A.n, rp, col[:nnz], val[:nnz], nnz)
+
+
+def dense_ewise_mult_masked(A, B, M: Csr, stream=None):
+    """C<M> = A .* B for dense m x n A, B (eWiseMult, include/matrix_la.h:189-208):
+    A(i,j)·B(i,j) on M's pattern, 0 elsewhere; returned like A."""
+    lib = _lib.load()
+    A, B = _dense(A), _dense(B)
+    m, n = A.shape
+    if tuple(B.shape) != (m, n):
+        raise ValueError("A and B must have the same shape")
+    C = _empty_like_space(A, (m, n), np.float64)
+    gm = M.as_gk()
+    check(lib.gk_dense_ewise_mult_masked(m, n, _ptr(A), _ptr(B), ctypes.byref(gm), _ptr(C), _stream(stream, A)))
+    return C
+
+
+def dense_fuse_ewise_mult_add(A, B, C, stream=None):
+    """C += A .* B elementwise, in place (fuseEWiseMultAdd,
+    include/matrix_la.h:182-187); C must be contiguous float64.  Returns C."""
+    lib = _lib.load()
+    A, B = _dense(A), _dense(B)
+    if (str(C.dtype) not in ("float64", "torch.float64")) or not (C.is_contiguous() if _is_torch(C)
+                                                                   else C.flags.c_contiguous):
+        raise ValueError("C must be a contiguous float64 array")
+    count = int(np.prod(tuple(C.shape)))
+    if int(np.prod(tuple(A.shape))) != count or int(np.prod(tuple(B.shape))) != count:
+        raise ValueError("A, B and C must have the same number of values")
+    check(lib.gk_dense_fuse_ewise_mult_add(count, _ptr(A), _ptr(B), _ptr(C), _stream(stream, C)))
+    return C
+
+
+def mxmm_spd(A: Csr, B, M: Csr, A_val=None, out=None, stream=None):
+    """C<M> = A·B with sparse A (m x k), dense B (k x n) and a dense result
+    that is 0 outside M (mxmm_spd, include/matrix_la.h:230-258).  A's values:
+    A_val (float64, nnz(A)) when given, else A.val, else 1.  `out` may be B
+    itself, as in the reference's mxmm_spd(Af, W, S, W, Wbuf)."""
+    lib = _lib.load()
+    B = _dense(B)
+    k, n = B.shape
+    if k != A.n:
+        raise ValueError("B must have A.n rows")
+    if A_val is not None:
+        A_val = _dense(A_val)
+    C = out if out is not None else _empty_like_space(B, (A.m, n), np.float64)
+    ga, gm = A.as_gk(), M.as_gk()
+    check(lib.gk_mxmm_spd(ctypes.byref(ga), _ptr(A_val), _ptr(B), n, ctypes.byref(gm), _ptr(C),
+                          _stream(stream, B, C)))
+    return C
+
+
 def tc_vertex(A: Csr, sched="plain", stream=None):
     """Triangles through each vertex of a symmetric adjacency
     (triangle_counting_vertex, src/main.cpp:16-39); int32 per vertex."""

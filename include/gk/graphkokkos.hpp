@@ -11,6 +11,8 @@
 //                       include/matrix_la.h:478-694, :936-1068 — C<M> = A·B, C
 //                       resized to M's pattern with explicit zeros kept (:564-568)
 //   mxmm_msa_cmask      include/matrix_la.h:733-934 — C<!M> = A·B
+//   add_nointersect / eWiseMult (dense, masked) / fuseEWiseMultAdd / mxmm_spd
+//                       include/matrix_la.h:182-328 (FP64 dense operands)
 //   triangle_counting_masked_sandia   src/main.cpp:69-90
 //   triangle_counting_vertex          src/main.cpp:16-39
 //   triangle_counting_masked_lu       src/main.cpp:42-66
@@ -204,6 +206,57 @@ void mxmm_msa_cmask(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &
     R.resizeVals(static_cast<size_t>(R.Rst(M.m)));
     gkb_detail::check(gk_mxmm_cmask(&a, &b, &mm, GK_PLUS_TIMES, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
     C = R;
+}
+
+// ----- operators of the alternate BC formulation (include/matrix_la.h:182-328) ---
+namespace gkb_detail {
+template <typename T>
+gk_csr pattern_of(const spMtx<T> &X) {
+    return gk_csr{static_cast<int64_t>(X.m), static_cast<int64_t>(X.n), static_cast<int64_t>(X.nz), X.Rst.data(),
+                  X.Col.data(), nullptr};
+}
+}  // namespace gkb_detail
+
+// C = A + B for non-intersecting patterns; the result lands in Cbuf and is
+// swapped into C, as the reference does (matrix_la.h:287-328).
+template <typename T>
+void add_nointersect(const spMtx<T> &A, const spMtx<T> &B, spMtx<T> &C, spMtx<T> &Cbuf) {
+    static_assert(std::is_same<T, int>::value, "add_nointersect takes int matrices (spMtx<int>)");
+    if (A.m != B.m || A.n != B.n) throw std::runtime_error("gk_b200: add_nointersect: shapes differ");
+    gk_csr a = A.csr(), b = B.csr();
+    spMtx<T> R(A.m, A.n, A.nz + B.nz);
+    gkb_detail::check(gk_add_nointersect(&a, &b, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
+    Cbuf = R;
+    std::swap(C, Cbuf);
+}
+
+// C<M> = A .* B on dense operands, 0 outside M (matrix_la.h:189-208).
+template <typename T, typename U>
+void eWiseMult(const denseMtx<T> &A, const denseMtx<T> &B, const spMtx<U> &M, denseMtx<T> &C) {
+    static_assert(std::is_same<T, double>::value, "the dense operators take denseMtx<double>");
+    gk_csr mm = gkb_detail::pattern_of(M);
+    gkb_detail::check(gk_dense_ewise_mult_masked(static_cast<int64_t>(C.m), static_cast<int64_t>(C.n), A.Val.data(),
+                                                 B.Val.data(), &mm, C.Val.data(), nullptr));
+}
+
+// C += A .* B (matrix_la.h:182-187).
+template <typename T>
+void fuseEWiseMultAdd(const denseMtx<T> &A, const denseMtx<T> &B, denseMtx<T> &C) {
+    static_assert(std::is_same<T, double>::value, "the dense operators take denseMtx<double>");
+    gkb_detail::check(gk_dense_fuse_ewise_mult_add(static_cast<int64_t>(A.m * A.n), A.Val.data(), B.Val.data(),
+                                                   C.Val.data(), nullptr));
+}
+
+// C<M> = A * B with sparse A, dense B and C (0 outside M); the product goes
+// through Cbuf and is swapped into C, as the reference does (matrix_la.h:230-258).
+template <typename T, typename U>
+void mxmm_spd(const spMtx<T> &A, const denseMtx<T> &B, const spMtx<U> &M, denseMtx<T> &C, denseMtx<T> &Cbuf) {
+    static_assert(std::is_same<T, double>::value, "mxmm_spd takes FP64 operands (spMtx<double>, denseMtx<double>)");
+    gk_csr a = gkb_detail::pattern_of(A), mm = gkb_detail::pattern_of(M);
+    if (Cbuf.m != C.m || Cbuf.n != C.n || Cbuf.Val.size() != C.m * C.n) Cbuf = denseMtx<T>(C.m, C.n);
+    gkb_detail::check(gk_mxmm_spd(&a, A.Val.data(), B.Val.data(), static_cast<int64_t>(B.n), &mm, Cbuf.Val.data(),
+                                  nullptr));
+    std::swap(C.Val, Cbuf.Val);
 }
 
 // ----- CSR transforms ------------------------------------------------------------

@@ -140,6 +140,37 @@ int gk_tc_row_sums(const gk_csr *L, uint64_t *row_sums, int sched, void *stream)
 int gk_mxmm_cmask(const gk_csr *A, const gk_csr *B, const gk_csr *M, int semiring, int64_t *C_rowptr,
                   int32_t *C_col, int32_t *C_val, void *stream);
 
+/* The operators of the reference's alternate (commented-out) BC formulation,
+ * include/betweenness_centrality.h:5-123.  Dense matrices are row-major FP64
+ * arrays (denseMtx, include/matrix.h:548-630: Val(i*n + j)); FP64 results
+ * are bit-exact with the reference, whose `x += a * b` is one fused
+ * multiply-add in its x86-64-v3 build. */
+
+/* C = A + B for matrices whose patterns do not intersect (add_nointersect,
+ * include/matrix_la.h:287-328): row i of C is the merge of A's and B's rows
+ * (on an equal column, which the operator does not expect, B's entry comes
+ * first).  C_rowptr (m+1) = A.rowptr + B.rowptr; C_col and C_val (may be
+ * NULL) hold nnz(A) + nnz(B) entries; pattern-only operands count as 1.  The
+ * reference's copy of a row's remaining B entries reads them at A's cursor
+ * (:320-322); C here is the true merge. */
+int gk_add_nointersect(const gk_csr *A, const gk_csr *B, int64_t *C_rowptr, int32_t *C_col, int32_t *C_val,
+                       void *stream);
+
+/* C<M> = A .* B on dense m x n operands (eWiseMult, include/matrix_la.h:189-208):
+ * C(i,j) = A(i,j) * B(i,j) where M has an entry, 0 elsewhere. */
+int gk_dense_ewise_mult_masked(int64_t m, int64_t n, const double *A, const double *B, const gk_csr *M, double *C,
+                               void *stream);
+
+/* C += A .* B over `count` values (fuseEWiseMultAdd, include/matrix_la.h:182-187). */
+int gk_dense_fuse_ewise_mult_add(int64_t count, const double *A, const double *B, double *C, void *stream);
+
+/* C<M> = A * B with sparse A (m x k), dense B (k x n) and dense C (m x n) that
+ * is 0 outside M's pattern (mxmm_spd, include/matrix_la.h:230-258).  A's
+ * values come from A_val (nnz(A) doubles) when given, else from A->val, else
+ * 1.  C may be B itself (the reference calls mxmm_spd(Af, W, S, W, Wbuf)). */
+int gk_mxmm_spd(const gk_csr *A, const double *A_val, const double *B, int64_t n, const gk_csr *M, double *C,
+                void *stream);
+
 /* Triangles through each vertex of a symmetric adjacency A:
  * counts[i] = (sum_j C(i,j)) >> 1 with C<A> = A·A, as int like the reference's
  * triangle_counting_vertex (src/main.cpp:16-39).  counts has A.m entries. */

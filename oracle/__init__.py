@@ -165,6 +165,89 @@ def ref_mxmm_cmask(A, B, M, parallel=True):
     return _cmask(ref().ref_mxmm_cmask, A, B, M, ctypes.c_int(1 if parallel else 0))
 
 
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a.cpu().numpy() if hasattr(a, "cpu") else a, dtype=np.float64))
+
+
+def _add_nointersect(fn, extra, A, B):
+    m, n, arp, acol, aval = _host(A)
+    _, _, brp, bcol, bval = _host(B)
+    nnz = int(arp[-1]) + int(brp[-1])
+    crp = np.zeros(m + 1, dtype=np.int64)
+    ccol = np.zeros(max(nnz, 1), dtype=np.int32)
+    cval = np.zeros(max(nnz, 1), dtype=np.int32)
+    if fn(*extra, _p(arp), _p(acol), _p(aval), _p(brp), _p(bcol), _p(bval), _p(crp), _p(ccol), _p(cval)) != 0:
+        raise ValueError("add_nointersect failed")
+    return crp, ccol[:nnz], cval[:nnz]
+
+
+def add_nointersect(A, B):
+    """C = A + B, the true merge (add_nointersect semantics): (rowptr, col, val)."""
+    return _add_nointersect(port().orc_add_nointersect, (I64(A.m),), A, B)
+
+
+def ref_add_nointersect(A, B):
+    """The reference's own add_nointersect (matrix_la.h:287-328); valid only
+    where every row's last entry comes from A."""
+    return _add_nointersect(ref().ref_add_nointersect, (I64(A.m), I64(A.n)), A, B)
+
+
+def _ewise(fn, A, B, M):
+    A, B = _f64(A), _f64(B)
+    m, n = A.shape
+    _, _, mrp, mcol, _ = _host(M)
+    C = np.empty((m, n), dtype=np.float64)
+    fn(I64(m), I64(n), _p(A), _p(B), _p(mrp), _p(mcol), _p(C))
+    return C
+
+
+def dense_ewise_mult_masked(A, B, M):
+    return _ewise(port().orc_dense_ewise_mult_masked, A, B, M)
+
+
+def ref_dense_ewise_mult_masked(A, B, M):
+    return _ewise(ref().ref_dense_ewise_mult_masked, A, B, M)
+
+
+def _fuse(fn, A, B, C):
+    A, B, C = _f64(A).ravel(), _f64(B).ravel(), _f64(C).ravel().copy()
+    fn(I64(C.size), _p(A), _p(B), _p(C))
+    return C
+
+
+def fuse_ewise_mult_add(A, B, C):
+    """C + A .* B (a new array)."""
+    return _fuse(port().orc_fuse_ewise_mult_add, A, B, C).reshape(np.shape(C))
+
+
+def ref_fuse_ewise_mult_add(A, B, C):
+    return _fuse(ref().ref_fuse_ewise_mult_add, A, B, C).reshape(np.shape(C))
+
+
+def mxmm_spd(A, B, M, A_val=None):
+    """C<M> = A·B with dense B, dense result (mxmm_spd semantics)."""
+    m, _, arp, acol, _ = _host(A)
+    B = _f64(B)
+    n = B.shape[1]
+    _, _, mrp, mcol, _ = _host(M)
+    av = None if A_val is None else _f64(A_val)
+    C = np.empty((m, n), dtype=np.float64)
+    port().orc_mxmm_spd(I64(m), _p(arp), _p(acol), _p(av), I64(n), _p(B), _p(mrp), _p(mcol), _p(C))
+    return C
+
+
+def ref_mxmm_spd(A, B, M, A_val=None):
+    """The reference's own mxmm_spd (matrix_la.h:230-258), FP64."""
+    m, k, arp, acol, _ = _host(A)
+    B = _f64(B)
+    n = B.shape[1]
+    _, _, mrp, mcol, _ = _host(M)
+    av = None if A_val is None else _f64(A_val)
+    C = np.empty((m, n), dtype=np.float64)
+    ref().ref_mxmm_spd(I64(m), I64(k), _p(arp), _p(acol), _p(av), I64(n), _p(B), _p(mrp), _p(mcol), _p(C))
+    return C
+
+
 def ktruss(A, k, record=64):
     m, _, rp, col, _ = _host(A)
     orp = np.zeros(m + 1, dtype=np.int64)

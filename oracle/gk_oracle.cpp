@@ -512,4 +512,71 @@ int orc_bc_f64(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *
     return 0;
 }
 
+// ---- operators of the alternate BC formulation (include/matrix_la.h:182-328) ----
+// FP64 sums use std::fma where the reference writes `x += a * b`, which its
+// x86-64-v3 build contracts into one fused multiply-add.
+
+// add_nointersect (matrix_la.h:287-328) as the true merge: c_rp = a_rp + b_rp;
+// row i takes A's entry while its column is smaller than B's, else B's (B
+// first on equal columns), then the rest of whichever row remains.  Values
+// of a pattern-only operand are 1.
+int orc_add_nointersect(int64_t m, const int64_t *arp, const int32_t *acol, const int32_t *aval,
+                        const int64_t *brp, const int32_t *bcol, const int32_t *bval, int64_t *crp, int32_t *ccol,
+                        int32_t *cval) {
+    for (int64_t i = 0; i <= m; ++i) crp[i] = arp[i] + brp[i];
+    for (int64_t i = 0; i < m; ++i) {
+        int64_t a = arp[i], b = brp[i], c = crp[i];
+        while (a < arp[i + 1] || b < brp[i + 1]) {
+            const bool take_a = b >= brp[i + 1] || (a < arp[i + 1] && acol[a] < bcol[b]);
+            if (take_a) {
+                ccol[c] = acol[a];
+                if (cval) cval[c] = aval ? aval[a] : 1;
+                ++a;
+            } else {
+                ccol[c] = bcol[b];
+                if (cval) cval[c] = bval ? bval[b] : 1;
+                ++b;
+            }
+            ++c;
+        }
+    }
+    return 0;
+}
+
+// Dense masked eWiseMult (matrix_la.h:189-208): C = 0, then C(i,j) = A(i,j)*B(i,j)
+// on M's pattern (row-major m x n).
+int orc_dense_ewise_mult_masked(int64_t m, int64_t n, const double *A, const double *B, const int64_t *mrp,
+                                const int32_t *mcol, double *C) {
+    std::fill(C, C + m * n, 0.0);
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t q = mrp[i]; q < mrp[i + 1]; ++q) {
+            const int64_t idx = i * n + mcol[q];
+            C[idx] = A[idx] * B[idx];
+        }
+    return 0;
+}
+
+// fuseEWiseMultAdd (matrix_la.h:182-187): C += A .* B.
+int orc_fuse_ewise_mult_add(int64_t count, const double *A, const double *B, double *C) {
+    for (int64_t i = 0; i < count; ++i) C[i] = std::fma(A[i], B[i], C[i]);
+    return 0;
+}
+
+// mxmm_spd (matrix_la.h:230-258): C = 0; for each A(i,j) in row order and each
+// column c of M's row i, C(i,c) += A(i,j) * B(j,c).  A's values: aval, else 1.
+int orc_mxmm_spd(int64_t m, const int64_t *arp, const int32_t *acol, const double *aval, int64_t n,
+                 const double *B, const int64_t *mrp, const int32_t *mcol, double *C) {
+    std::fill(C, C + m * n, 0.0);
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t q = arp[i]; q < arp[i + 1]; ++q) {
+            const double a = aval ? aval[q] : 1.0;
+            const int64_t j = acol[q];
+            for (int64_t k = mrp[i]; k < mrp[i + 1]; ++k) {
+                const int64_t c = mcol[k];
+                C[i * n + c] = std::fma(a, B[j * n + c], C[i * n + c]);
+            }
+        }
+    return 0;
+}
+
 }  // extern "C"

@@ -131,6 +131,23 @@ spMtx<int> k_truss_fixed(const spMtx<int> &A, int k, mxmOp<int> matrixMult, bool
     return C;
 }
 
+spMtx<double> make_mtx_d(int64_t m, int64_t n, const int64_t *rp, const int32_t *col, const double *val) {
+    const int64_t nz = rp[m];
+    spMtx<double> A(static_cast<size_t>(m), static_cast<size_t>(n), static_cast<size_t>(nz));
+    for (int64_t i = 0; i <= m; ++i) A.Rst(i) = static_cast<int>(rp[i]);
+    for (int64_t j = 0; j < nz; ++j) {
+        A.Col(j) = col[j];
+        A.Val(j) = val ? val[j] : 1.0;
+    }
+    return A;
+}
+
+denseMtx<double> make_dense(int64_t m, int64_t n, const double *v) {
+    denseMtx<double> D(static_cast<size_t>(m), static_cast<size_t>(n));
+    for (int64_t i = 0; i < m * n; ++i) D.Val(i) = v[i];
+    return D;
+}
+
 void export_csr(const spMtx<int> &R, int64_t *rp, int32_t *col, int32_t *val) {
     for (size_t i = 0; i <= R.m; ++i) rp[i] = R.Rst(i);
     for (size_t j = 0; j < R.nz; ++j) {
@@ -194,6 +211,55 @@ int ref_mxmm_cmask(int parallel,
     } catch (...) {
         return -1;
     }
+}
+
+// The reference's add_nointersect (matrix_la.h:287-328).  It sizes its result
+// by the output's row count and loops over it (:295-299), so C starts with m
+// rows.  Its copy of a row's remaining B entries reads B at A's cursor
+// (:320-322): call it only where every row's last entry comes from A.
+int ref_add_nointersect(int64_t m, int64_t n, const int64_t *arp, const int32_t *acol, const int32_t *aval,
+                        const int64_t *brp, const int32_t *bcol, const int32_t *bval, int64_t *crp, int32_t *ccol,
+                        int32_t *cval) {
+    try {
+        spMtx<int> A = make_mtx(m, n, arp, acol, aval);
+        spMtx<int> B = make_mtx(m, n, brp, bcol, bval);
+        spMtx<int> C(static_cast<size_t>(m), static_cast<size_t>(n)), Cbuf;
+        add_nointersect(A, B, C, Cbuf);
+        export_csr(C, crp, ccol, cval);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// The reference's dense masked eWiseMult (matrix_la.h:189-208).
+int ref_dense_ewise_mult_masked(int64_t m, int64_t n, const double *A, const double *B, const int64_t *mrp,
+                                const int32_t *mcol, double *C) {
+    denseMtx<double> a = make_dense(m, n, A), b = make_dense(m, n, B), c(static_cast<size_t>(m), static_cast<size_t>(n));
+    spMtx<int> M = make_mtx(m, n, mrp, mcol, nullptr);
+    eWiseMult(a, b, M, c);
+    for (int64_t i = 0; i < m * n; ++i) C[i] = c.Val(i);
+    return 0;
+}
+
+// The reference's fuseEWiseMultAdd (matrix_la.h:182-187) on a 1 x count matrix.
+int ref_fuse_ewise_mult_add(int64_t count, const double *A, const double *B, double *C) {
+    denseMtx<double> a = make_dense(1, count, A), b = make_dense(1, count, B), c = make_dense(1, count, C);
+    fuseEWiseMultAdd(a, b, c);
+    for (int64_t i = 0; i < count; ++i) C[i] = c.Val(i);
+    return 0;
+}
+
+// The reference's mxmm_spd (matrix_la.h:230-258) with FP64 values.
+int ref_mxmm_spd(int64_t m, int64_t k, const int64_t *arp, const int32_t *acol, const double *aval, int64_t n,
+                 const double *B, const int64_t *mrp, const int32_t *mcol, double *C) {
+    spMtx<double> A = make_mtx_d(m, k, arp, acol, aval);
+    denseMtx<double> b = make_dense(k, n, B);
+    spMtx<int> M = make_mtx(m, n, mrp, mcol, nullptr);
+    denseMtx<double> c(static_cast<size_t>(m), static_cast<size_t>(n)), cbuf(static_cast<size_t>(m), static_cast<size_t>(n));
+    mxmm_spd(A, b, M, c, cbuf);
+    for (int64_t i = 0; i < m * n; ++i) C[i] = c.Val(i);
+    return 0;
 }
 
 // Triangle count of a symmetric adjacency matrix (sorted rows, no self-loops).

@@ -60,7 +60,31 @@ int main(int argc, char **argv) {
     mxmm_msa_cmask(true, A, A, A, NC);
     long long ncsum = 0;
     for (size_t j = 0; j < NC.nz; ++j) ncsum += NC.Val(j);
-    std::printf("{\"scale\": %d, \"seed\": %llu, \"nnz\": %zu, \"tc_msa\": %lld, \"tc_mca\": %lld, \"tc_user\": %lld, "
+    // the alternate-BC operators: L + U merges back into A (disjoint patterns);
+    // W = A·1 on A's pattern gives every entry of row i the degree of i
+    spMtx<int> U = transpose(L), LU, LUbuf;
+    add_nointersect(L, U, LU, LUbuf);
+    const bool add_ok = (LU == A);
+    spMtx<double> Ad(A.m, A.n, A.nz);
+    for (size_t i = 0; i <= A.m; ++i) Ad.Rst(i) = A.Rst(i);
+    for (size_t j = 0; j < A.nz; ++j) {
+        Ad.Col(j) = A.Col(j);
+        Ad.Val(j) = 1.0;
+    }
+    denseMtx<double> W(A.m, A.m), Wbuf, Sq(A.m, A.m);
+    for (size_t i = 0; i < A.m * A.m; ++i) W.Val(i) = 1.0;
+    mxmm_spd(Ad, W, A, W, Wbuf);
+    bool spd_ok = true;
+    for (size_t i = 0; i < A.m && spd_ok; ++i)
+        for (int64_t q = A.Rst(i); q < A.Rst(i + 1); ++q)
+            if (W.Val(i * A.m + A.Col(q)) != static_cast<double>(A.Rst(i + 1) - A.Rst(i))) spd_ok = false;
+    eWiseMult(W, W, A, Sq);   // deg(i)^2 on A's pattern
+    fuseEWiseMultAdd(W, W, Sq);  // + deg(i)^2 again
+    double sqsum = 0;
+    for (size_t i = 0; i < A.m * A.m; ++i) sqsum += Sq.Val(i);
+    std::printf("{\"add_nointersect_ok\": %s, \"spd_ok\": %s, \"ewise_sum\": %.17g, ",
+                add_ok ? "true" : "false", spd_ok ? "true" : "false", sqsum);
+    std::printf("\"scale\": %d, \"seed\": %llu, \"nnz\": %zu, \"tc_msa\": %lld, \"tc_mca\": %lld, \"tc_user\": %lld, "
                 "\"mxm_sum\": %lld, \"ktruss_nnz\": %zu, \"ktruss_iters\": %d, \"bc_float_sum\": %.9g, "
                 "\"bc_f64_sum\": %.17g, \"symm_roundtrip\": %s, \"transpose_nnz\": %s, \"vertex_sum\": %lld, "
                 "\"tc_lu\": %lld, \"cmask_nnz\": %zu, \"cmask_sum\": %lld}\n",

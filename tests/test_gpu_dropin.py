@@ -43,3 +43,6 @@ def test_dropin_matches_oracle(dropin_exe, gk, orc, cuda, scale, seed):
     crp, ccol, cval = orc.mxmm_cmask(A, A, A)
     assert res["cmask_nnz"] == len(ccol) and res["cmask_sum"] == int(cval.astype(np.int64).sum())
     assert res["vertex_sum"] == int(orc.ref_tc_vertex(A).astype(np.int64).sum())
+    assert res["add_nointersect_ok"] and res["spd_ok"]
+    deg = np.diff(np.asarray(A.rowptr)).astype(np.float64)
+    assert res["ewise_sum"] == float(2.0 * np.sum(deg ** 3))  # deg(i)^2 on deg(i) entries, twice

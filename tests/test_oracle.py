@@ -263,3 +263,75 @@ def test_cmask_vs_reference(orc, seed):
     S = G.random_csr(120, 120, 0.05, seed=seed)
     for w, g in zip(orc.ref_mxmm_cmask(S, S, S, parallel=False), orc.mxmm_cmask(S, S, S)):
         np.testing.assert_array_equal(w, g)
+
+
+# ---------------------------------------------------------------------------
+# operators of the alternate BC formulation (include/matrix_la.h:182-328)
+# ---------------------------------------------------------------------------
+def disjoint_pair(m, n, seed, density=0.15):
+    """Sparse A, B (m x n, int values) with disjoint patterns; every row of A
+    ends at column n-1, which B never uses, so no row ends with B entries
+    (the reference's B-tail copy is then not reached)."""
+    rng = np.random.default_rng(seed)
+    pick = rng.random((m, n - 1)) < density
+    side = rng.random((m, n - 1)) < 0.5
+    a = np.zeros((m, n), dtype=bool)
+    a[:, : n - 1] = pick & side
+    a[:, n - 1] = True
+    b = np.zeros((m, n), dtype=bool)
+    b[:, : n - 1] = pick & ~side
+
+    def csr(mask):
+        r, c = np.nonzero(mask)
+        rp = np.zeros(m + 1, dtype=np.int64)
+        np.cumsum(np.bincount(r, minlength=m), out=rp[1:])
+        return G.Csr(m, n, rp, c.astype(np.int32), rng.integers(-9, 10, len(c)).astype(np.int32), len(c))
+    return csr(a), csr(b)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_add_nointersect_vs_reference(orc, seed):
+    need_ref(orc)
+    A, B = disjoint_pair(70, 40, seed)
+    for w, g in zip(orc.ref_add_nointersect(A, B), orc.add_nointersect(A, B)):
+        np.testing.assert_array_equal(w, g)
+
+
+def test_add_nointersect_closed_form(orc):
+    # row 0 ends with B entries (the case the reference mis-copies), row 1 is
+    # B only, row 2 A only, row 3 empty
+    A = G.Csr(4, 5, np.array([0, 1, 1, 3, 3]), np.array([1, 0, 4], dtype=np.int32),
+              np.array([10, 20, 30], dtype=np.int32), 3)
+    B = G.Csr(4, 5, np.array([0, 3, 5, 5, 5]), np.array([0, 2, 3, 1, 4], dtype=np.int32),
+              np.array([1, 2, 3, 4, 5], dtype=np.int32), 5)
+    rp, col, val = orc.add_nointersect(A, B)
+    np.testing.assert_array_equal(rp, [0, 4, 6, 8, 8])
+    np.testing.assert_array_equal(col, [0, 1, 2, 3, 1, 4, 0, 4])
+    np.testing.assert_array_equal(val, [1, 10, 2, 3, 4, 5, 20, 30])
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_dense_operators_vs_reference(orc, seed):
+    """The dense masked eWiseMult, fuseEWiseMultAdd and mxmm_spd of the
+    reference against the restatement, bit for bit (FP64)."""
+    need_ref(orc)
+    rng = np.random.default_rng(seed)
+    m, k, n = 37, 29, 45
+    A = rng.standard_normal((m, n))
+    B = rng.standard_normal((m, n))
+    C = rng.standard_normal((m, n))
+    M = G.random_csr(m, n, 0.2, seed=seed)
+    np.testing.assert_array_equal(orc.ref_dense_ewise_mult_masked(A, B, M), orc.dense_ewise_mult_masked(A, B, M))
+    np.testing.assert_array_equal(orc.ref_fuse_ewise_mult_add(A, B, C), orc.fuse_ewise_mult_add(A, B, C))
+    S = G.random_csr(m, k, 0.25, seed=seed + 1)
+    sval = rng.standard_normal(S.nnz)
+    D = rng.standard_normal((k, n))
+    np.testing.assert_array_equal(orc.ref_mxmm_spd(S, D, M, sval), orc.mxmm_spd(S, D, M, sval))
+    np.testing.assert_array_equal(orc.ref_mxmm_spd(S, D, M), orc.mxmm_spd(S, D, M))
+    # closed form: a pattern-only A sums B's rows; the mask selects columns
+    want = np.zeros((m, n))
+    dense_s = G.dense_of(S) != 0
+    for i in range(m):
+        cols = np.asarray(M.col[M.rowptr[i]:M.rowptr[i + 1]])
+        want[i, cols] = D[dense_s[i]].sum(axis=0)[cols]
+    np.testing.assert_allclose(orc.mxmm_spd(S, D, M), want, rtol=1e-12, atol=1e-12)
