@@ -50,6 +50,17 @@ def rank_info():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def job_rate(torch, units_per_rank, ms, dist, world, device="cuda"):
+    """Whole-job throughput of weak-scaled replicas: every rank processes
+    units_per_rank per step; the job's step time is the slowest rank's
+    (max-reduced over the ranks).  Returns (units per second, max ms)."""
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return units_per_rank * world / (ms_max / 1e3), ms_max
+
+
 def hbm_peak():
     try:
         with open(PEAKS_PATH) as f:
@@ -237,11 +248,8 @@ def run_tc(args, wl, torch, gk, dist, rank, world):
         c = int(out.item())
         assert count is None or c == count, "schedulers disagree"
         count = c
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        res[sched] = {"value": L.nnz * world / (ms_max / 1e3), "ms_per_step": ms_max}
+        rate, ms_max = job_rate(torch, L.nnz, ms, dist, world)
+        res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
     line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
@@ -344,11 +352,8 @@ def run_ktruss(args, wl, torch, gk, dist, rank, world):
         sig = (state["it"], T.nnz, int(T.col.sum().item()))
         assert ref is None or sig == ref, "schedulers disagree"
         ref = sig
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        res[sched] = {"value": (A.nnz // 2) * world / (ms_max / 1e3), "ms_per_step": ms_max}
+        rate, ms_max = job_rate(torch, (A.nnz // 2), ms, dist, world)
+        res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
     edges = A.nnz // 2
     line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
@@ -442,11 +447,8 @@ def run_bc(args, wl, torch, gk, dist, rank, world):
             ref = got
         else:
             assert np.allclose(got, ref, rtol=1e-12, atol=1e-9), "schedulers disagree"
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        res[sched] = {"value": traversed * world / (ms_max / 1e3), "ms_per_step": ms_max}
+        rate, ms_max = job_rate(torch, traversed, ms, dist, world)
+        res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
     line = {"metric": METRIC, "value": res[head]["value"], "unit": "TEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
@@ -527,11 +529,8 @@ def run_tcbatch(args, wl, torch, gk, dist, rank, world):
             clk = clocks.stop()
         assert ref is None or np.array_equal(out[0], ref), "schedulers disagree"
         ref = out[0]
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        res[sched] = {"value": nnz * world / (ms_max / 1e3), "ms_per_step": ms_max}
+        rate, ms_max = job_rate(torch, nnz, ms, dist, world)
+        res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
     line = {"metric": METRIC, "value": res[head]["value"], "unit": "edges/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],

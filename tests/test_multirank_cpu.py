@@ -1,0 +1,84 @@
+"""The N>1 plumbing of bench.py on CPU: two ranks over gloo (127.0.0.1).  The
+workloads are weak-scaled replicas (no data-path collective), so what has to
+hold across ranks is the timing rule — the job's step time is the slowest
+rank's — and the whole-job throughput built from it; the reference arm runs
+on rank 0 only and the other ranks exit without work."""
+import io
+import json
+import os
+import socket
+import sys
+from contextlib import redirect_stdout
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as td
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    td.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ms = 10.0 * (rank + 1)  # rank 1 is the slow one
+        rate, ms_max = bench.job_rate(torch, 1000, ms, td, world, device="cpu")
+        td.barrier()
+        out.put((rank, rate, ms_max))
+    finally:
+        td.destroy_process_group()
+
+
+def test_job_rate_takes_the_slowest_rank():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    got = sorted(q.get() for _ in range(world))
+    for rank, rate, ms_max in got:
+        assert ms_max == 20.0  # the max over ranks, on every rank
+        assert rate == pytest.approx(1000 * world / 0.020)
+
+
+def test_job_rate_single_process():
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    rate, ms = bench.job_rate(torch, 500, 4.0, None, 1, device="cpu")
+    assert (rate, ms) == (500 / 0.004, 4.0)
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    args = type("Args", (), {"workload": "tc14", "steps": 1, "warmup": 1, "gpus": 2})()
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.main_reference(args)
+    assert buf.getvalue() == ""
+    # rank 0 of the same job prints the line (k-truss: its documented unavailable line)
+    monkeypatch.setenv("RANK", "0")
+    args.workload = "ktruss20"
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.main_reference(args)
+    line = json.loads(buf.getvalue())
+    assert line["impl"] == "reference" and "unavailable" in line
