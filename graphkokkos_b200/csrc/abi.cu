@@ -40,6 +40,49 @@ static int check_square_pattern(const gk_csr *L, const char *name) {
     return GK_OK;
 }
 
+// A side stream for host-to-device copies that run ahead of the caller's
+// stream, with one event per stage.  Released on every return path; the
+// caller's stream first waits for the side stream, so that scratch freed in
+// order on the caller's stream outlives every copy into it.
+struct CopyPipe {
+    cudaStream_t s, cs = nullptr;
+    std::vector<cudaEvent_t> ev;
+    explicit CopyPipe(cudaStream_t s_) : s(s_) {}
+    CopyPipe(const CopyPipe &) = delete;
+    CopyPipe &operator=(const CopyPipe &) = delete;
+    // creates the side stream and `stages` + 1 events; the last one orders the
+    // side stream after the work already queued on the caller's stream
+    int open(int stages) {
+        GK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        ev.resize(static_cast<size_t>(stages) + 1, nullptr);
+        for (auto &e : ev) GK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        GK_CUDA(cudaEventRecord(ev[stages], s));
+        GK_CUDA(cudaStreamWaitEvent(cs, ev[stages], 0));
+        return GK_OK;
+    }
+    // the caller's stream waits for the copies queued so far as stage q
+    int stage_done(int q) {
+        GK_CUDA(cudaEventRecord(ev[q], cs));
+        GK_CUDA(cudaStreamWaitEvent(s, ev[q], 0));
+        return GK_OK;
+    }
+    ~CopyPipe() {
+        if (cs) {
+            cudaEvent_t done;
+            if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+                cudaEventRecord(done, cs);
+                cudaStreamWaitEvent(s, done, 0);
+                cudaEventDestroy(done);
+            } else {
+                cudaStreamSynchronize(cs);
+            }
+        }
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        if (cs) cudaStreamDestroy(cs);
+    }
+};
+
 static int tc_common(const gk_csr *L, int epi, unsigned long long *dev_sums, int sched, cudaStream_t s,
                      Scratch &scr, int force_variant = -1) {
     DevCsr d;
@@ -463,37 +506,11 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
     gstart.push_back(ngraphs);
     const int ngroups = static_cast<int>(gstart.size()) - 1;
 
-    // side stream and events, released on every return path; the caller's
-    // stream first waits for the side stream, so that the scratch (freed in
-    // order on the caller's stream) outlives every copy into it
-    struct Pipe {
-        cudaStream_t s, cs = nullptr;
-        std::vector<cudaEvent_t> ev;
-        explicit Pipe(cudaStream_t s_) : s(s_) {}
-        ~Pipe() {
-            if (cs) {
-                cudaEvent_t done;
-                if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
-                    cudaEventRecord(done, cs);
-                    cudaStreamWaitEvent(s, done, 0);
-                    cudaEventDestroy(done);
-                } else {
-                    cudaStreamSynchronize(cs);
-                }
-            }
-            for (cudaEvent_t e : ev)
-                if (e) cudaEventDestroy(e);
-            if (cs) cudaStreamDestroy(cs);
-        }
-    } pipe(s);
+    CopyPipe pipe(s);
     cudaStream_t cs = s;
     if (any_host && ngroups > 1) {
-        GK_CUDA(cudaStreamCreateWithFlags(&pipe.cs, cudaStreamNonBlocking));
+        GK_CHECK(pipe.open(ngroups));  // after the buffers' allocation and the sums' zeroing
         cs = pipe.cs;
-        pipe.ev.resize(ngroups + 1, nullptr);
-        for (auto &e : pipe.ev) GK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        GK_CUDA(cudaEventRecord(pipe.ev[ngroups], s));  // buffers allocated, sums zeroed
-        GK_CUDA(cudaStreamWaitEvent(cs, pipe.ev[ngroups], 0));
     }
     for (int q = 0; q < ngroups; ++q) {
         const int g0 = gstart[q], g1 = gstart[q + 1];
@@ -505,10 +522,7 @@ int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int
                     GK_CUDA(cudaMemcpyAsync(col + slots[g].ebase, graphs[g].col, sizeof(int32_t) * graphs[g].nnz,
                                             cudaMemcpyDefault, cs));
             }
-            if (cs != s) {
-                GK_CUDA(cudaEventRecord(pipe.ev[q], cs));
-                GK_CUDA(cudaStreamWaitEvent(s, pipe.ev[q], 0));
-            }
+            if (cs != s) GK_CHECK(pipe.stage_done(q));
         }
         const int64_t v0 = slots[g0].vbase, e0 = slots[g0].ebase;
         const int64_t v1 = g1 < ngraphs ? slots[g1].vbase : vtot, e1 = g1 < ngraphs ? slots[g1].ebase : etot;
