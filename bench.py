@@ -191,18 +191,25 @@ def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None):
     achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
     return {"kernel": f"masked SpGEMM variant {dom}", "bound": "hbm", "achieved": round(achieved, 1),
             "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic_for(dom), "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
+            "traffic": traffic_for(dom, d["work"]), "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
             "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "rows": x["rows"]}
                          for v, x in sorted(per.items())}}
 
 
-def traffic_for(variant):
+def traffic_for(variant, work):
+    """DRAM bytes (read + write) of one launch of `variant` streaming `work`
+    B entries: the full-size ncu capture of that kernel on the same graph
+    (profiles/tc_rmat24_traffic.json), scaled by the streamed entries when the
+    schedule has since moved rows onto or off the variant."""
     path = os.path.join(ROOT, "profiles", "tc_rmat24_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(str(variant))
+            rec = json.load(f).get(str(variant))
     except Exception:
         return None
+    if not rec or not rec.get("work"):
+        return None
+    return int(round(rec["traffic"] * work / rec["work"]))
 
 
 def cpu_baseline(L_host, target_s=12.0):
