@@ -23,6 +23,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -79,17 +80,19 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        self.lines = []
+        self.reader = None
 
     def start(self):
         try:
-            self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+        self.reader = threading.Thread(target=lambda: self.lines.extend(self.proc.stdout), daemon=True)
+        self.reader.start()
 
     def stop(self):
         if self.proc is None:
@@ -100,10 +103,10 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        self.f.close()
+        self.reader.join(timeout=5)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in list(self.lines):
             p = [x.strip() for x in line.split(",")]
             if len(p) < 9:
                 continue
@@ -115,7 +118,6 @@ class ClockSampler:
             for n, v in zip(names, p[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
-        os.remove(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
@@ -152,11 +154,12 @@ def time_steps(torch, fn, steps, warmup, dist=None):
     return e0.elapsed_time(e1) / steps
 
 
-def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None):
+def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None, traffic_key=None):
     """Per-variant CUDA-event durations of one profiled call (work totals)
     plus events-only brackets over timed calls; the dominant variant's
     algorithmic bytes per launch divided by its mean launch time.  `call`
-    runs the product (default: gk_tc_count on L into a device counter)."""
+    runs the product (default: gk_tc_count on L into a device counter);
+    traffic_key names the workload whose ncu capture gives `traffic`."""
     lib = gk.load()
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
     if call is None:
@@ -189,9 +192,10 @@ def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None):
     dom = max(per, key=lambda v: per[v]["ms"])
     d = per[dom]
     achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9
+    traffic = traffic_for(dom, d["work"]) if traffic_key == "tc24" else None
     return {"kernel": f"masked SpGEMM variant {dom}", "bound": "hbm", "achieved": round(achieved, 1),
             "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic_for(dom, d["work"]), "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
+            "traffic": traffic, "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
             "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "rows": x["rows"]}
                          for v, x in sorted(per.items())}}
 
@@ -270,7 +274,7 @@ def run_tc(args, wl, torch, gk, dist, rank, world):
             "triangles": count, "schedulers": res, "gpu_launches": launches, "clocks": clk}
     if rank == 0:
         peak, peak_kind = hbm_peak()
-        line["roofline"] = tc_roofline(gk, torch, L, head, peak, peak_kind)
+        line["roofline"] = tc_roofline(gk, torch, L, head, peak, peak_kind, traffic_key=args.workload)
         # end to end through the public API with host buffers: the H2D copy of
         # L (pinned) and the D2H read of the count are inside the timed region
         Lh = L.to("cpu")

@@ -91,3 +91,24 @@ def test_roofline_traffic_scales_with_streamed_entries():
     assert bench.traffic_for(6, rec["work"]) == rec["traffic"]  # the captured launch itself
     assert bench.traffic_for(6, rec["work"] // 2) == pytest.approx(rec["traffic"] / 2, rel=1e-9)
     assert bench.traffic_for(3, 10) is None  # no capture of that kernel
+
+
+def test_clock_sampler_parses_nvidia_smi_lines(tmp_path, monkeypatch):
+    """The clock sampler reads nvidia-smi's CSV from a pipe; a stand-in
+    executable prints two samples, one of them with sw_power_cap active."""
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\n"
+                    "echo '0, 1965, 1965, 700.5, 0x0, Not Active, Not Active, Not Active, Not Active'\n"
+                    "echo '0, 1800, 1965, 990.1, 0x4, Not Active, Not Active, Not Active, Active'\n"
+                    "sleep 30\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ['PATH']}")
+    sys.path.insert(0, ROOT)
+    import time
+
+    import bench
+    c = bench.ClockSampler(0)
+    c.start()
+    time.sleep(0.5)
+    got = c.stop()
+    assert got == {"sm_mhz": 1882.5, "sm_max_mhz": 1965.0, "samples": 2, "reasons": ["sw_power_cap"]}
