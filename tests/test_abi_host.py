@@ -139,3 +139,32 @@ def test_lower_host(gk, orc):
     orp, ocol = orc.extract_lower(A)
     np.testing.assert_array_equal(L.rowptr, orp)
     np.testing.assert_array_equal(L.col, ocol)
+
+
+def test_dense_operator_arguments_are_checked_before_any_call(gk):
+    """The Python operators refuse mismatched dense shapes and a non-float64
+    in-place output before reaching the library (no GPU needed)."""
+    from tests import graphs as G
+    M = G.random_csr(4, 5, 0.5, seed=1)
+    with pytest.raises(ValueError):
+        gk.dense_ewise_mult_masked(np.zeros((4, 5)), np.zeros((4, 6)), M)
+    with pytest.raises(ValueError):
+        gk.dense_fuse_ewise_mult_add(np.zeros(6), np.zeros(6), np.zeros(6, dtype=np.float32))
+    with pytest.raises(ValueError):
+        gk.dense_fuse_ewise_mult_add(np.zeros(6), np.zeros(5), np.zeros(6))
+    S = G.random_csr(4, 3, 0.5, seed=2)
+    with pytest.raises(ValueError):
+        gk.mxmm_spd(S, np.zeros((4, 5)), M)  # B must have S.n = 3 rows
+
+
+def test_c_abi_refuses_bad_arguments_without_a_gpu(gk):
+    """Shape and null-pointer errors come back as GK_ERR_ARG from the host
+    side of the C ABI, before any device work."""
+    lib = gk.load()
+    A = gk.Csr(3, 3, np.array([0, 1, 2, 3]), np.array([1, 2, 0], dtype=np.int32), None, 3).as_gk()
+    B = gk.Csr(4, 4, np.zeros(5, dtype=np.int64), np.zeros(0, dtype=np.int32), None, 0).as_gk()
+    rp = np.zeros(4, dtype=np.int64)
+    assert lib.gk_add_nointersect(ctypes.byref(A), ctypes.byref(B), rp.ctypes.data, None, None, None) == 1
+    assert lib.gk_mxmm_spd(ctypes.byref(A), None, None, 2, ctypes.byref(B), None, None) == 1
+    assert lib.gk_dense_ewise_mult_masked(-1, 2, None, None, ctypes.byref(A), None, None) == 1
+    assert b"shape" in lib.gk_last_error_string() or b"negative" in lib.gk_last_error_string()
