@@ -12,13 +12,16 @@
 //  3. sched_choose  one variant per bin (plain heuristic or learned MLP)
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
 //                   get their item count (mask chunks x A-entry splits)
-//  5. one persistent kernel per variant over its rows / items:
-//       HASH_GROUP  G in {4,8,16,32} threads per row, the mask row's columns in a
-//                   shared-memory hash set (slot = accumulator)
+//  5. one persistent kernel per variant over its rows / items (the catalogue
+//     of 17 variants is the table in gk_sched.cuh):
+//       HASH_GROUP  4, 8 or 32 threads per row, the mask row's columns in a
+//                   shared-memory bucketed hash set (slot = accumulator)
 //       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
 //                   binary search (mask-compressed accumulator, matrix_la.h:437-461)
-//       HASH_BLOCK  one CTA per item, 8K/32K-slot hash set, warps take A entries
-//                   dynamically; heavy rows split over several CTAs
+//       HASH_BLOCK  one CTA per item (row x mask chunk x A-entry split), a
+//                   512- to 16K-slot table, warps take A entries dynamically;
+//                   a bitmap filter in front of the table, or none (every
+//                   element looked up), or an exact map of the low columns
 //       MCA_BLOCK   one CTA per item, up to 16K sorted mask columns
 //       MSA_BLOCK   one CTA per item, dense column-window accumulator
 //                   (the reference's MSA, matrix_la.h:611-631) or bitmap
