@@ -100,7 +100,7 @@ def test_clock_sampler_parses_nvidia_smi_lines(tmp_path, monkeypatch):
     fake.write_text("#!/bin/sh\n"
                     "echo '0, 1965, 1965, 700.5, 0x0, Not Active, Not Active, Not Active, Not Active'\n"
                     "echo '0, 1800, 1965, 990.1, 0x4, Not Active, Not Active, Not Active, Active'\n"
-                    "sleep 30\n")
+                    "exec sleep 30\n")
     fake.chmod(0o755)
     monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ['PATH']}")
     sys.path.insert(0, ROOT)
