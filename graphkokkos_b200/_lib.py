@@ -132,6 +132,7 @@ SIGNATURES = {
     "gk_launch_count": (ctypes.c_int64, []),
     "gk_last_error_string": (ctypes.c_char_p, []),
     "gk_version": (ctypes.c_int, []),
+    "gk_inject_alloc_failure": (ctypes.c_int, [ctypes.c_int64]),
 }
 
 _lib = None

@@ -59,8 +59,21 @@ Context &ctx() {
     return c;
 }
 
+// Allocation-failure injection for testing error paths (gk_inject_alloc_failure):
+// the countdown's allocation fails once, -1 is off.
+static std::atomic<long long> g_alloc_countdown{-1};
+
+static bool injected_alloc_failure() {
+    long long c = g_alloc_countdown.load(std::memory_order_relaxed);
+    while (c >= 0) {
+        if (g_alloc_countdown.compare_exchange_weak(c, c - 1, std::memory_order_relaxed)) return c == 0;
+    }
+    return false;
+}
+
 int Scratch::raw_alloc(void **p, size_t bytes) {
     if (n_ >= 64) return fail(GK_ERR_OOM, "internal: too many scratch allocations in one call");
+    if (injected_alloc_failure()) return fail(GK_ERR_OOM, "injected allocation failure (gk_inject_alloc_failure)");
     bytes = (bytes + 255) & ~size_t(255);
     if (bytes == 0) bytes = 256;
     if (arena_) {
@@ -530,3 +543,8 @@ int64_t gk_launch_count(void) { return gk::g_launches.load(); }
 extern "C" const char *gk_last_error_string(void) { return gk::g_last_error.c_str(); }
 
 extern "C" int gk_version(void) { return 100; }
+
+extern "C" int gk_inject_alloc_failure(int64_t after) {
+    gk::g_alloc_countdown.store(after < 0 ? -1 : static_cast<long long>(after), std::memory_order_relaxed);
+    return GK_OK;
+}

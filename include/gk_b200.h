@@ -364,6 +364,13 @@ int64_t gk_launch_count(void);
 const char *gk_last_error_string(void);
 int gk_version(void);
 
+/* Test hook for error paths: after the next `after` scratch allocations of
+ * this process (device or fixed-arena), the following one fails once with
+ * GK_ERR_OOM; a negative value switches it off.  No counterpart in the
+ * reference; it lets tests drive every allocation failure of an operator and
+ * check that the library stays usable, without exhausting device memory. */
+int gk_inject_alloc_failure(int64_t after);
+
 #ifdef __cplusplus
 }
 #endif
