@@ -423,6 +423,7 @@ int gk_tc_count_lu(const gk_csr *A, uint64_t *count, int sched, void *stream) {
 }
 
 int gk_tc_count_batched(const gk_csr *graphs, int ngraphs, uint64_t *counts, int sched, void *stream) {
+    NvtxRange range("gk:tc_count_batched");
     if (ngraphs < 0 || (ngraphs > 0 && (!graphs || !counts))) return fail(GK_ERR_ARG, "bad batch arguments");
     if (ngraphs == 0) return GK_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -1152,6 +1152,7 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const B
 // Validates A and the sources, stages them, runs the batch.
 static int bc_entry(const gk_csr *A, const int32_t *sources, int nsources, double *bc, const BcOptions &opt,
                     void *stream) {
+    NvtxRange range("gk:bc_batch");
     GK_CHECK(validate_csr_shape(A, "A"));
     if (A->m != A->n) return fail(GK_ERR_ARG, "non-square matrix; BC is only for square matrices");
     if (nsources < 0 || (nsources > 0 && !sources) || (A->m > 0 && !bc)) return fail(GK_ERR_ARG, "bad arguments");

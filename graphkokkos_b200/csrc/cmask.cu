@@ -119,6 +119,7 @@ using namespace gk;
 
 extern "C" int gk_mxmm_cmask(const gk_csr *A, const gk_csr *B, const gk_csr *M, int semiring, int64_t *C_rowptr,
                              int32_t *C_col, int32_t *C_val, void *stream) {
+    NvtxRange range("gk:mxmm_cmask");
     GK_CHECK(validate_csr_shape(A, "A"));
     GK_CHECK(validate_csr_shape(B, "B"));
     GK_CHECK(validate_csr_shape(M, "M"));

@@ -330,6 +330,7 @@ static bool csr_check_enabled() {
 
 int check_csr_batch(const DevCsr &d, int64_t ebase, int64_t row_base, const int32_t *key, const int64_t *estart,
                     const unsigned int *pre_flags, int level, const char *name, cudaStream_t s, Scratch &scr) {
+    NvtxRange range("gk:csr_check");
     if (level <= 0 || !csr_check_enabled()) return GK_OK;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {

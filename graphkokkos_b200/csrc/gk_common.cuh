@@ -8,6 +8,7 @@
 #include <string>
 
 #include "../../include/gk_b200.h"
+#include <nvtx3/nvToolsExt.h>  // header-only; ranges are no-ops unless a profiler is attached
 
 namespace gk {
 
@@ -121,6 +122,15 @@ SideStreams &side_streams();
 
 // ----- launch counter and per-variant profiling (gk_launch_count, gk_prof_*) ----
 void note_launches(int n);
+
+// An NVTX range around a phase of an operator (nsys timelines, ncu --nvtx
+// filters); costs nothing measurable when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 bool prof_enabled();
 bool prof_any();          // any profiling mode (its events cannot be captured into graphs)
 int64_t launches_noted();  // kernel launches counted so far

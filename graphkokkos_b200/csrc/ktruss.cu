@@ -266,6 +266,7 @@ static int ktruss_graph(const KtBuffers &b, cudaStream_t s, int *passes_per_laun
 
 int ktruss_device(int64_t m, int64_t nnz0, int64_t *rp_a, int32_t *col_a, int k, int sched, int *iters_out,
                   int64_t *nnz_out, int64_t **rp_res, int32_t **col_res, cudaStream_t s, Scratch &scr) {
+    NvtxRange range("gk:ktruss");
     *rp_res = rp_a;
     *col_res = col_a;
     if (nnz0 == 0 || m == 0) {  // the reference counts one pass over the empty matrix

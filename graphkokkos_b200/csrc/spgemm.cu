@@ -713,10 +713,17 @@ size_t spgemm_scratch_bytes(int64_t m) {
            r(4 * NBINS) + r(4 * (6 * NV + 4)) + r(4 * NV) + r(tmp_bytes);
 }
 
+// NVTX range names of the variant launches
+static const char *const kVariantRange[NV] = {
+    "gk:variant 0",  "gk:variant 1",  "gk:variant 2",  "gk:variant 3",  "gk:variant 4",  "gk:variant 5",
+    "gk:variant 6",  "gk:variant 7",  "gk:variant 8",  "gk:variant 9",  "gk:variant 10", "gk:variant 11",
+    "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16"};
+
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
 int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
+    NvtxRange range("gk:masked_spgemm");
     const DevCsr &A = rq.A, &B = rq.B, &M = rq.M;
     if (A.m != M.m || A.n != B.m || B.n != M.n)
         return fail(GK_ERR_ARG, "shape mismatch: need A.m == M.m, A.n == B.m, B.n == M.n");
@@ -826,6 +833,7 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
             vs = side.s[v];
             GK_CUDA(cudaStreamWaitEvent(vs, side.fork, 0));
         }
+        NvtxRange vrange(kVariantRange[v]);
         prof.begin(v, vs);
         cudaError_t e = launch_variant(v, args, rq.epi, val, sms, vs);
         if (e != cudaSuccess) return cuda_fail(e, "masked SpGEMM variant launch");
