@@ -1,5 +1,6 @@
-// The reference-side adapter of INTEGRATION.md section 1, verbatim in its
-// logic: an mxmOp-compatible mxmm_b200 over the reference's own spMtx (its
+// The reference-side adapter of the integration guide, with the plain
+// scheduler (which needs no model): an mxmOp-compatible mxmm_b200 over the
+// reference's own spMtx (its
 // include/matrix.h, compiled here against the Kokkos-API shim of oracle/),
 // plus the fused entry points called with spMtx storage.  Compiled and linked
 // against libgk_b200.so by tests/test_ref_adapter_cpu.py; run with an
