@@ -6,7 +6,7 @@
  * (triangle counting, k-truss, batched betweenness centrality).  The
  * reference exposes these as C++ templates over host-resident Kokkos Views;
  * this header exposes the same operations with plain pointers and sizes so
- * that any host language can bind them (see INTEGRATION.md).
+ * that any host language can bind them.
  *
  * Conventions
  *  - Matrices are CSR: int64 row pointers (m+1), int32 column indices sorted
