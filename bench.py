@@ -221,7 +221,7 @@ def cpu_baseline(L_host, target_s=12.0):
     strided row sample of L, on this host's cores; falls back to the port."""
     import oracle
     kind = "reference" if oracle.ref_available() else "port"
-    stride = 4096
+    stride = min(4096, max(1, L_host.m // 64))  # a first sample of at least 64 rows
     cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
     # grow the sample toward ~target_s seconds of CPU work
     if sec > 0:
@@ -717,7 +717,7 @@ def main_reference(args):
     kind = "reference" if oracle.ref_available() else "port"
     # size the per-step sample so that warmup + steps stay within a few minutes
     per_step_budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
-    stride = 1 << 14
+    stride = min(1 << 14, max(1, L.m // 64))  # a first sample of at least 64 rows
     _, nz, sec, thr = oracle.tc_row_stride(L, stride, 0, kind=kind)
     if sec > 0:
         stride = max(1, min(stride, int(stride * sec / per_step_budget)))
