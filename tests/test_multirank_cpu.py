@@ -112,3 +112,23 @@ def test_clock_sampler_parses_nvidia_smi_lines(tmp_path, monkeypatch):
     time.sleep(0.5)
     got = c.stop()
     assert got == {"sm_mhz": 1882.5, "sm_max_mhz": 1965.0, "samples": 2, "reasons": ["sw_power_cap"]}
+
+
+def test_reference_arm_on_a_small_workload(monkeypatch):
+    """`bench.py --impl reference` on triangle counting RMAT-14: the sampled
+    reference rows (never an empty sample, which the reference's mxmm_msa
+    cannot take) give a positive rate and the contract's keys."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference oracle not built")
+    monkeypatch.setenv("RANK", "0")
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    args = type("Args", (), {"workload": "tc14", "steps": 2, "warmup": 1, "gpus": 1})()
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.main_reference(args)
+    line = json.loads(buf.getvalue())
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "edges/s"
+    assert line["cpu_baseline"]["kind"] == "reference" and line["e2e"]["h2d_bytes_per_step"] == 0
