@@ -249,7 +249,11 @@ def forward_numpy(w, X, nf, nv):
     return h2 @ W3.T + b3
 
 
-LEARNED_MARGIN = 0.1375  # log2(1.1): the model must predict >= 10% gain over the plain pick
+# log2(1.1): the model must predict >= 10% gain over the plain pick.  The row-bin
+# scheduler's margin follows GK_LEARNED_MARGIN as the library's does; the BC
+# level chooser's is fixed.
+BC_LEARNED_MARGIN = 0.1375
+LEARNED_MARGIN = float(os.environ.get("GK_LEARNED_MARGIN", BC_LEARNED_MARGIN))
 
 
 def choose(out, recs):
@@ -363,11 +367,11 @@ def bc_dataset(recs):
 
 def bc_choose(out, recs):
     """The plain rule's shape unless the model predicts the other one
-    LEARNED_MARGIN (log2) faster (as k_bc_choose does)."""
+    BC_LEARNED_MARGIN (log2) faster (as k_bc_choose does)."""
     picks = []
     for o, r in zip(out, recs):
         p = r["plain"]
-        picks.append(1 - p if o[p] - o[1 - p] >= LEARNED_MARGIN else p)
+        picks.append(1 - p if o[p] - o[1 - p] >= BC_LEARNED_MARGIN else p)
     return picks
 
 
