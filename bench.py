@@ -216,22 +216,58 @@ def traffic_for(variant, work):
     return int(round(rec["traffic"] * work / rec["work"]))
 
 
+GOLDEN_LARGE = os.path.join(ROOT, "tests", "golden", "large.json")
+
+
+def golden_large(kind, **match):
+    """The oracle's answer for this workload from tests/golden/large.json
+    (tests/golden/make_golden_large.py), or None when it holds none."""
+    if not os.path.exists(GOLDEN_LARGE):
+        return None
+    for case in json.load(open(GOLDEN_LARGE)).get(kind, []):
+        if all(case.get(k) == v for k, v in match.items()):
+            return case
+    return None
+
+
+def tc_sampler(L_host, kind, target_s):
+    """Stride of a row sample of L whose reference TC takes about target_s
+    seconds on this host's cores.  A first sample of about 64 rows runs twice
+    (the first also faults in the per-thread scratch pool, as Kokkos' pool
+    would be warm in a long run); its second time and entry count give the
+    per-entry rate the stride is sized from.  Returns (stride, probe)."""
+    import oracle
+    stride = max(1, L_host.m // 64)
+    oracle.tc_row_stride(L_host, stride, 0, kind=kind)
+    cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
+    probe = {"rows": (L_host.m + stride - 1) // stride, "entries": nz, "seconds": sec}
+    if sec > 0 and nz > 0:
+        stride = max(1, min(stride, int(stride * sec / target_s)))
+    return stride, probe
+
+
 def cpu_baseline(L_host, target_s=12.0):
     """The reference's mxmm_msa (oracle/_ref, via the Kokkos-API shim) on a
-    strided row sample of L, on this host's cores; falls back to the port."""
+    strided row sample of L, on this host's cores; falls back to the port.
+    The sample is compacted to its rows, so the reference's per-call costs
+    that scale with the row count follow the sample (oracle/ref_oracle.cpp,
+    ref_tc_row_stride)."""
     import oracle
     kind = "reference" if oracle.ref_available() else "port"
-    stride = min(4096, max(1, L_host.m // 64))  # a first sample of at least 64 rows
+    stride, probe = tc_sampler(L_host, kind, target_s)
     cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
-    # grow the sample toward ~target_s seconds of CPU work
-    if sec > 0:
-        want = max(1, int(stride * sec / target_s))
-        stride = max(16, min(stride, want))
-        if stride < 4096:
-            cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
     return {"value": nz / sec if sec > 0 else None, "unit": "edges/s", "cores": thr, "kind": kind,
             "sample": f"rows i % {stride} == 0 of L ({nz} of {L_host.nnz} entries), {sec:.1f} s, "
-                      f"C<S> = S·L then sum (reference bracket src/main.cpp:74-85)"}
+                      f"C<S> = S·L then sum (reference bracket src/main.cpp:74-85); a {probe['rows']}-row "
+                      f"sample ({probe['entries']} entries) took {probe['seconds']:.3f} s"}
+
+
+def tc_config(wl, m, nnz_lower):
+    """The workload's identity, the same in both arms' lines."""
+    return {"workload": f"triangle counting C<L>=L·L on RMAT-{wl['scale']} seed {wl['seed']}",
+            "scale": wl["scale"], "edge_factor": 16, "seed": wl["seed"], "vertices": m, "nnz_lower": nnz_lower,
+            "rowptr": "int64",
+            "l2": f"inputs larger than L2 (L = {nnz_lower * 4 / 1e9:.2f} GB of columns, no flush needed)"}
 
 
 def run_tc(args, wl, torch, gk, dist, rank, world):
@@ -267,11 +303,13 @@ def run_tc(args, wl, torch, gk, dist, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic: seeded RMAT (a,b,c,d=.57,.19,.19,.05, edge factor 16, no noise/permutation), "
                     "symmetrised, self-loops and duplicates removed, generated on the device",
-            "config": {"workload": f"triangle counting C<L>=L·L on RMAT-{scale} seed {seed}",
-                       "scale": scale, "edge_factor": 16, "seed": seed, "vertices": L.m, "nnz_lower": L.nnz,
-                       "rowptr": "int64", "sched": head, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": f"inputs larger than L2 (L = {L.nnz * 4 / 1e9:.2f} GB of columns, no flush needed)"},
+            "config": tc_config(wl, L.m, L.nnz), "sched": head,
+            "parallelism": "replicas" if world > 1 else "single",
             "triangles": count, "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    gold = golden_large("tc", scale=scale, seed=seed)
+    if gold is not None:
+        assert count == gold["triangles"], ("oracle disagrees", count, gold["triangles"])
+        line["parity"] = {"oracle": "tests/golden/large.json", "triangles": gold["triangles"], "equal": True}
     if rank == 0:
         peak, peak_kind = hbm_peak()
         line["roofline"] = tc_roofline(gk, torch, L, head, peak, peak_kind, traffic_key=args.workload)
@@ -363,6 +401,11 @@ def run_ktruss(args, wl, torch, gk, dist, rank, world):
         sig = (state["it"], T.nnz, int(T.col.sum().item()))
         assert ref is None or sig == ref, "schedulers disagree"
         ref = sig
+        gold = golden_large("ktruss", scale=wl["scale"], seed=wl["seed"], k=wl["k"])
+        if gold is not None:
+            from tests.golden.make_golden import edge_hash
+            h = edge_hash(T.rowptr.cpu().numpy(), T.col[:T.nnz].cpu().numpy())
+            assert (state["it"], T.nnz, h) == (gold["iterations"], gold["nnz"], gold["xor_hash"]), "oracle disagrees"
         rate, ms_max = job_rate(torch, (A.nnz // 2), ms, dist, world)
         res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
@@ -376,6 +419,9 @@ def run_ktruss(args, wl, torch, gk, dist, rank, world):
                        "loop": "one CUDA graph per call (conditional while node around a captured pass)",
                        "l2": "inputs larger than L2 (support SpGEMM streams > 100 GB per pass)"},
             "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if gold is not None:
+        line["parity"] = {"oracle": "tests/golden/large.json", "iterations": gold["iterations"], "nnz": gold["nnz"],
+                          "edge_hash": gold["xor_hash"], "equal": True}
     if rank == 0:
         peak, peak_kind = hbm_peak()
         line["roofline"] = ktruss_roofline(gk, torch, A, wl["k"], head, peak, peak_kind)
@@ -395,6 +441,14 @@ def run_ktruss(args, wl, torch, gk, dist, rank, world):
     return line
 
 
+def bc_agree(got, want, rtol=1e-12):
+    """FP64 BC scores within rtol relative; exact zeros must stay exact."""
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    zero = want == 0.0
+    return bool(np.all(np.where(zero, got == 0.0, np.abs(got - want) <= rtol * np.abs(want))))
+
+
 def bc_traversed(A, src):
     """Undirected edges in each source's component, summed over the sources
     (the TEPS numerator), and the directed edges of those components."""
@@ -406,6 +460,14 @@ def bc_traversed(A, src):
     ncomp, lab = cg.connected_components(M, directed=False)
     directed_per_comp = np.bincount(lab[np.repeat(np.arange(A.m), np.diff(rp))], minlength=ncomp)
     return int((directed_per_comp[lab[src]] // 2).sum()), int(directed_per_comp[lab[src]].sum())
+
+
+def bc_config(wl, m, nnz):
+    """The BC workload's identity, the same in both arms' lines."""
+    return {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources",
+            "scale": wl["scale"], "seed": wl["seed"], "sources": wl["nsrc"], "source_seed": wl["src_seed"],
+            "vertices": m, "nnz": nnz,
+            "l2": f"sigma and R arrays of {2 * m * wl['nsrc'] * 8 / 1e9:.1f} GB exceed L2"}
 
 
 def bc_cpu_baseline(A, nsample=8, seed=7):
@@ -457,7 +519,12 @@ def run_bc(args, wl, torch, gk, dist, rank, world):
         if ref is None:
             ref = got
         else:
-            assert np.allclose(got, ref, rtol=1e-12, atol=1e-9), "schedulers disagree"
+            assert bc_agree(got, ref), "schedulers disagree"
+        gold = golden_large("bc", scale=wl["scale"], seed=wl["seed"], nsrc=wl["nsrc"], src_seed=wl["src_seed"])
+        if gold is not None:
+            idx = np.asarray(gold["spot_index"])
+            assert bc_agree(got[idx], np.asarray(gold["spot_value"])), "oracle disagrees"
+            assert int((got == 0.0).sum()) == gold["zeros"], "oracle disagrees"
         rate, ms_max = job_rate(torch, traversed, ms, dist, world)
         res[sched] = {"value": rate, "ms_per_step": ms_max}
     head = scheds[-1]
@@ -466,13 +533,14 @@ def run_bc(args, wl, torch, gk, dist, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded RMAT (a,b,c,d=.57,.19,.19,.05, edge factor 16), generated on the device; "
                     f"{wl['nsrc']} sources sampled uniformly (seed {wl['src_seed']})",
-            "config": {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources",
-                       "vertices": A.m, "nnz": A.nnz, "sched": head,
-                       "teps_numerator": "undirected edges in each source's component, summed over sources",
-                       "teps_all_edges": (A.nnz // 2) * len(src) / (res[head]["ms_per_step"] / 1e3),
-                       "loop": "forward and backward levels as CUDA graphs (conditional while nodes)",
-                       "l2": f"sigma and R arrays of {2 * A.m * 512 * 8 / 1e9:.1f} GB exceed L2"},
+            "config": bc_config(wl, A.m, A.nnz), "sched": head,
+            "teps_numerator": "undirected edges in each source's component, summed over sources",
+            "teps_all_edges": (A.nnz // 2) * len(src) / (res[head]["ms_per_step"] / 1e3),
+            "loop": "forward and backward levels as CUDA graphs (conditional while nodes)",
             "schedulers": res, "gpu_launches": launches, "clocks": clk}
+    if gold is not None:
+        line["parity"] = {"oracle": "tests/golden/large.json", "spot_scores": len(gold["spot_index"]),
+                          "rtol": 1e-12, "atol": 0, "zeros": gold["zeros"], "equal": True}
     if rank == 0:
         peak, peak_kind = hbm_peak()
         # algorithmic bytes: 8 B of sigma per (directed edge, source) in the
@@ -494,13 +562,20 @@ def run_bc(args, wl, torch, gk, dist, rank, world):
         for _ in range(e2e_steps):
             bh = gk.bc_batch(Ah, src, sched=head)
         e2e_s = (time.perf_counter() - t0) / e2e_steps
-        assert np.allclose(np.asarray(bh), ref, rtol=1e-12, atol=1e-9)
+        assert bc_agree(np.asarray(bh), ref)
         line["e2e"] = {"value": traversed / e2e_s, "unit": "TEPS", "ms_per_step": e2e_s * 1e3,
                        "h2d_bytes_per_step": 8 * (A.m + 1) + 4 * A.nnz + 4 * len(src),
                        "d2h_bytes_per_step": 8 * A.m, "api": "gk_bc_batch with pinned host CSR arrays"}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = bc_cpu_baseline(A)
     return line
+
+
+def batch_config(wl):
+    """The many-graph workload's identity, the same in both arms' lines."""
+    return {"workload": f"many-graph triangle counting, {wl['ngraphs']} graphs (half ER, half RMAT-10..17), "
+                        f"seeds {wl['seed0']}..{wl['seed0'] + wl['ngraphs'] - 1}, one batched call",
+            "graphs": wl["ngraphs"], "seed0": wl["seed0"]}
 
 
 def build_batch(gk, torch, specs):
@@ -547,11 +622,9 @@ def run_tcbatch(args, wl, torch, gk, dist, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res[head]["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic: seeded Erdos-Renyi and RMAT graphs generated on the device",
-            "config": {"workload": f"many-graph triangle counting, {len(Ls)} graphs (half ER, half RMAT-10..17), "
-                                   f"seeds {wl['seed0']}..{wl['seed0'] + len(Ls) - 1}, one batched call",
-                       "graphs": len(Ls), "nnz_lower_total": nnz, "vertices_total": sum(L.m for L in Ls),
-                       "sched": head, "triangles_total": int(ref.sum()),
-                       "l2": f"inputs larger than L2 ({nnz * 4 / 1e9:.2f} GB of columns)"},
+            "config": batch_config(wl), "sched": head, "graphs": len(Ls), "nnz_lower_total": nnz,
+            "vertices_total": sum(L.m for L in Ls), "triangles_total": int(ref.sum()),
+            "l2": f"inputs larger than L2 ({nnz * 4 / 1e9:.2f} GB of columns)",
             "schedulers": res, "gpu_launches": launches, "clocks": clk}
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -633,11 +706,10 @@ def reference_bc(args, wl, world):
     the workload's sources per step (relabelled to 0..b-1, as it takes them),
     one thread (its row split is unsafe with more)."""
     import oracle
-    import graphkokkos_b200 as gk
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled here) not built"}))
         return
-    A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"])
+    A = oracle.gen_rmat(wl["scale"], 16, wl["seed"])
     src = np.random.default_rng(wl["src_seed"]).choice(A.m, size=wl["nsrc"], replace=False)
     per = 4
     vals = []
@@ -653,7 +725,7 @@ def reference_bc(args, wl, world):
     v = statistics.median(vals)
     print(json.dumps(reference_line(
         args, wl, world, v, "TEPS",
-        {"workload": f"batched BC, RMAT-{wl['scale']} seed {wl['seed']}, {wl['nsrc']} sources", "sched": "n/a"},
+        bc_config(wl, A.m, A.nnz),
         "reference", 1, f"each step: {per} of the workload's sources, reference BC (float), one thread")))
 
 
@@ -661,17 +733,17 @@ def reference_tcbatch(args, wl, world):
     """The reference's triangle count (mxmm_msa, oracle/_ref) on whole graphs
     of the batch, a different slice of graphs per step, on the host's cores."""
     import oracle
-    import graphkokkos_b200 as gk
+    from graphkokkos_b200.api import uneven_batch_specs  # parameters only: the library is not loaded
     kind = "reference" if oracle.ref_available() else "port"
-    specs = gk.api.uneven_batch_specs(wl["ngraphs"], wl["seed0"])
+    specs = uneven_batch_specs(wl["ngraphs"], wl["seed0"])
     vals = []
     thr = 1
     for i in range(args.warmup + args.steps):
         nz_tot, sec_tot = 0, 0.0
         for g in range(i, len(specs), 97):
             kind_g, a, b, seed = specs[g]
-            A = gk.gen_rmat(a, b, seed=seed) if kind_g == "rmat" else gk.gen_er(a, b, seed=seed)
-            _, nz, sec, thr = oracle.tc_row_stride(gk.lower_host(A), 1, 0, kind=kind)
+            Lg = oracle.gen_rmat(a, b, seed, lower=True) if kind_g == "rmat" else oracle.gen_er(a, b, seed, lower=True)
+            _, nz, sec, thr = oracle.tc_row_stride(Lg, 1, 0, kind=kind)
             nz_tot += nz
             sec_tot += sec
             if sec_tot > max(2.0, 120.0 / max(1, args.steps + args.warmup)):
@@ -681,7 +753,7 @@ def reference_tcbatch(args, wl, world):
     v = statistics.median(vals)
     print(json.dumps(reference_line(
         args, wl, world, v, "edges/s",
-        {"workload": f"many-graph triangle counting, {wl['ngraphs']} graphs", "sched": "n/a"},
+        batch_config(wl),
         kind, thr, "each step: whole graphs g = step, step+97, ... of the batch until ~the step's time budget; "
                    "the reference's mxmm_msa + sum per graph")))
 
@@ -691,7 +763,6 @@ def main_reference(args):
     if rank != 0:
         return
     import oracle
-    import graphkokkos_b200 as gk
     wl = WORKLOADS[args.workload]
     if wl["kind"] == "bc":
         return reference_bc(args, wl, world)
@@ -702,26 +773,15 @@ def main_reference(args):
                           "k-truss is not sampleable: the reference's whole loop on RMAT-20 takes tens of minutes "
                           "on the host cores (11 passes of its support product)"}))
         return
-    try:
-        import torch
-        dev = "cuda" if torch.cuda.is_available() else "cpu"
-    except Exception:
-        dev = "cpu"
-    # input generation is not timed; the GPU builder is used when present
-    if dev == "cuda":
-        A = gk.gen_rmat(wl["scale"], 16, seed=wl["seed"], device="cuda")
-        L = gk.extract_lower(A).numpy()
-        del A
-    else:
-        L = gk.lower_host(gk.gen_rmat(wl["scale"], 16, seed=wl["seed"]))
+    # input generation (not timed) with the oracle's own restatement of the
+    # seeded generator: the product library is not loaded in this arm
+    L = oracle.gen_rmat(wl["scale"], 16, wl["seed"], lower=True)
     kind = "reference" if oracle.ref_available() else "port"
     # size the per-step sample so that warmup + steps stay within a few minutes
     per_step_budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
-    stride = min(1 << 14, max(1, L.m // 64))  # a first sample of at least 64 rows
-    _, nz, sec, thr = oracle.tc_row_stride(L, stride, 0, kind=kind)
-    if sec > 0:
-        stride = max(1, min(stride, int(stride * sec / per_step_budget)))
+    stride, probe = tc_sampler(L, kind, per_step_budget)
     vals = []
+    thr = 1
     for i in range(args.warmup + args.steps):
         cnt, nz, sec, thr = oracle.tc_row_stride(L, stride, i % stride, kind=kind)
         if i >= args.warmup:
@@ -729,11 +789,13 @@ def main_reference(args):
     v = statistics.median(vals)
     line = {"metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic: seeded RMAT", "impl": "reference",
-            "config": {"workload": f"triangle counting C<L>=L·L on RMAT-{wl['scale']} seed {wl['seed']}",
-                       "scale": wl["scale"], "seed": wl["seed"], "nnz_lower": L.nnz},
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic: seeded RMAT (oracle restatement of the "
+            "generator, bit-identical to the library's)", "impl": "reference",
+            "config": tc_config(wl, L.m, L.nnz), "sched": "n/a",
             "cpu_baseline": {"value": v, "unit": "edges/s", "cores": thr, "kind": kind,
-                             "sample": f"each step: rows i % {stride} == offset of L, reference mxmm_msa + sum"},
+                             "sample": f"each step: rows i % {stride} == offset of L (compacted), reference "
+                                       f"mxmm_msa + sum; a {probe['rows']}-row sample took "
+                                       f"{probe['seconds']:.3f} s"},
             "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

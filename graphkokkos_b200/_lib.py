@@ -96,6 +96,8 @@ SIGNATURES = {
     "gk_bc_batch": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, VP, ctypes.c_int, VP]),
     "gk_extract_lower": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, VP, c_i64p, VP]),
     "gk_transpose": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, VP, VP, VP]),
+    "gk_build_symm_from_lower": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, VP, VP, VP]),
+    "gk_build_adjacency_matrix": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, VP, VP, VP]),
     "gk_gen_rmat": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_uint64, c_i64p, VP, VP, VP]),
     "gk_gen_er": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64, c_i64p, VP, VP, VP]),
@@ -113,6 +115,7 @@ SIGNATURES = {
     "gk_sched_num_features": (ctypes.c_int, []),
     "gk_sched_model_size": (ctypes.c_size_t, []),
     "gk_sched_set_model": (ctypes.c_int, [VP, ctypes.c_size_t]),
+    "gk_sched_load_model_file": (ctypes.c_int, [ctypes.c_char_p]),
     "gk_sched_has_model": (ctypes.c_int, []),
     "gk_sched_num_bins": (ctypes.c_int, []),
     "gk_sched_variant_allowed": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
@@ -122,6 +125,7 @@ SIGNATURES = {
     "gk_mlp_train": (ctypes.c_int, [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_float, VP, VP]),
     "gk_mlp_forward": (ctypes.c_int, [VP, VP, ctypes.c_int, VP, VP]),
     "gk_bc_set_model": (ctypes.c_int, [VP, ctypes.c_size_t]),
+    "gk_bc_load_model_file": (ctypes.c_int, [ctypes.c_char_p]),
     "gk_bc_has_model": (ctypes.c_int, []),
     "gk_bc_tune": (ctypes.c_int, [ctypes.POINTER(GkCsr), VP, ctypes.c_int, ctypes.c_int, VP, VP, VP, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_int), VP]),

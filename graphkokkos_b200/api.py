@@ -349,6 +349,31 @@ def transpose(A: Csr, with_values=False, stream=None) -> Csr:
     return Csr(A.n, A.m, rp, col[:A.nnz], None if val is None else val[:A.nnz], A.nnz)
 
 
+def build_symm_from_lower(L: Csr, with_values=False, stream=None) -> Csr:
+    """Symmetric matrix merged from L and transpose(L) on the GPU
+    (build_symm_from_lower, include/matrix.h:662-696)."""
+    lib = _lib.load()
+    nnz = 2 * L.nnz
+    rp = _empty_like_space(L.rowptr, (L.m + 1,), np.int64)
+    col = _empty_like_space(L.col, (max(nnz, 1),), np.int32)
+    val = _empty_like_space(L.col, (max(nnz, 1),), np.int32) if with_values else None
+    g = L.as_gk()
+    check(lib.gk_build_symm_from_lower(ctypes.byref(g), _ptr(rp), _ptr(col), _ptr(val), _stream(stream, L.col)))
+    return Csr(L.m, L.n, rp, col[:nnz], None if val is None else val[:nnz], nnz)
+
+
+def build_adjacency_matrix(G: Csr, stream=None) -> Csr:
+    """G's pattern with every value 1, on the GPU (build_adjacency_matrix,
+    include/matrix.h:643-660)."""
+    lib = _lib.load()
+    rp = _empty_like_space(G.rowptr, (G.m + 1,), np.int64)
+    col = _empty_like_space(G.col, (max(G.nnz, 1),), np.int32)
+    val = _empty_like_space(G.col, (max(G.nnz, 1),), np.int32)
+    g = G.as_gk()
+    check(lib.gk_build_adjacency_matrix(ctypes.byref(g), _ptr(rp), _ptr(col), _ptr(val), _stream(stream, G.col)))
+    return Csr(G.m, G.n, rp, col[:G.nnz], val[:G.nnz], G.nnz)
+
+
 # ---------------------------------------------------------------------------
 # graph generation
 # ---------------------------------------------------------------------------

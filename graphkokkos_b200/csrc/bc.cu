@@ -45,12 +45,12 @@
 #include <vector>
 
 #include "gk_common.cuh"
+#include "gk_internal_host.h"
 #include "gk_device.cuh"
 #include "gk_sched.cuh"
 
 namespace gk {
 
-int transpose_device(const DevCsr &A, int64_t *orp, int32_t *ocol, int32_t *oval, cudaStream_t s, Scratch &scr);
 
 // Widest chunk: 32 * GK_BC_TMAX sources (a power of two, at most 16).
 #ifndef GK_BC_TMAX
@@ -1226,6 +1226,13 @@ extern "C" int gk_bc_set_model(const float *weights, size_t n_floats) {
     g_bc_model.assign(weights, weights + n_floats);
     ++g_bc_model_version;
     return GK_OK;
+}
+
+extern "C" int gk_bc_load_model_file(const char *path) {
+    std::vector<float> w;
+    const std::string err = read_model_file(path, w);
+    if (!err.empty()) return fail(GK_ERR_ARG, "gk_bc_load_model_file: " + err);
+    return gk_bc_set_model(w.data(), w.size());
 }
 
 extern "C" int gk_bc_has_model(void) {

@@ -108,6 +108,11 @@ int stage_csr(const gk_csr *in, DevCsr *out, Scratch &scr, cudaStream_t s, int64
 bool is_device_pointer(const void *p);
 int validate_csr_shape(const gk_csr *c, const char *name);
 
+// Device CSR transforms (abi.cu): the transpose (A.n + 1 row pointers out,
+// rows sorted; oval may be null) and the strict lower triangle.
+int transpose_device(const DevCsr &A, int64_t *orp, int32_t *ocol, int32_t *oval, cudaStream_t s, Scratch &scr);
+int extract_lower_device(const DevCsr &A, int64_t *orp, int32_t *ocol, cudaStream_t s, Scratch &scr);
+
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 // ----- side streams for concurrent kernel variants ----------------------------

@@ -1,6 +1,7 @@
 // Host-side internal types shared by the library's C++ translation units.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <vector>
 
 struct gk_host_graph {
@@ -12,3 +13,11 @@ struct gk_host_graph {
     std::vector<int32_t> val;  // read from a file that carries values (has_val)
     bool has_val = false;
 };
+
+namespace gk {
+// Reads a scheduler model file: the 8 bytes "GKMLP001", a little-endian
+// uint32 count, then count little-endian float32 weights (written by
+// graphkokkos_b200/sched.py).  Returns an empty string on success, else what
+// was wrong with the file.
+std::string read_model_file(const char *path, std::vector<float> &out);
+}  // namespace gk

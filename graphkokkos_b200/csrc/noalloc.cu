@@ -42,21 +42,24 @@ constexpr size_t GK_NOALLOC_BYTES = size_t(36) << 20;
 // bin table, counters, the scan's temporary storage and the accumulator.
 static __device__ __align__(256) unsigned char g_tc_scratch[GK_NOALLOC_BYTES];
 
+constexpr int GK_NOALLOC_MAX_DEVICES = 64;
 static std::mutex g_noalloc_mutex;
-static void *g_noalloc_ptr[64];
+static void *g_noalloc_ptr[GK_NOALLOC_MAX_DEVICES];
 
 // Device address of g_tc_scratch on the current device (set up once per device).
 static int noalloc_arena(void **out) {
     int dev = 0;
     GK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= GK_NOALLOC_MAX_DEVICES)
+        return fail(GK_ERR_UNSUPPORTED, "gk_tc_count_noalloc: device ordinals above 63 are not supported");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev & 63]) {
+    if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_tc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_tc_scratch)");
-        g_noalloc_ptr[dev & 63] = p;
+        g_noalloc_ptr[dev] = p;
     }
-    *out = g_noalloc_ptr[dev & 63];
+    *out = g_noalloc_ptr[dev];
     return GK_OK;
 }
 
@@ -70,7 +73,8 @@ extern "C" int gk_tc_count_noalloc(const gk_csr *L, uint64_t *count, int sched, 
     if (!count) return fail(GK_ERR_ARG, "count is null");
     if (L->m > GK_NOALLOC_MAX_ROWS)
         return fail(GK_ERR_ARG, "gk_tc_count_noalloc: L has more than 1048576 rows, the limit of its fixed scratch");
-    if ((L->m > 0 && !is_device_pointer(L->rowptr)) || (L->nnz > 0 && !is_device_pointer(L->col)))
+    // the row pointers are read on the device even for an empty graph (rowptr[0], rowptr[m])
+    if (!is_device_pointer(L->rowptr) || (L->nnz > 0 && !is_device_pointer(L->col)))
         return fail(GK_ERR_ARG, "gk_tc_count_noalloc: L must be in device memory (staging host arrays would allocate)");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     void *arena = nullptr;

@@ -191,6 +191,85 @@ extern "C" int gk_add_nointersect(const gk_csr *A, const gk_csr *B, int64_t *C_r
     return GK_OK;
 }
 
+// build_symm_from_lower (include/matrix.h:662-696): the reference merges row
+// i of Low with row i of Upp = transpose(Low), Upp first on equal columns.
+// That is add_nointersect(Low, Upp) with the same tie rule, so the device
+// path is the transpose (radix sort by column) and the two placement passes.
+extern "C" int gk_build_symm_from_lower(const gk_csr *L, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
+                                        void *stream) {
+    GK_CHECK(validate_csr_shape(L, "L"));
+    if (L->m != L->n) return fail(GK_ERR_ARG, "build_symm_from_lower: L must be square");
+    const int64_t m = L->m, nnz = 2 * L->nnz;
+    if (!out_rowptr || (nnz > 0 && !out_col)) return fail(GK_ERR_ARG, "build_symm_from_lower: null output");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scr(s);
+    DevCsr low;
+    GK_CHECK(stage_csr(L, &low, scr, s, nullptr, CSR_SORTED, "L"));
+    DevCsr up{m, m, low.nnz, nullptr, nullptr, nullptr};
+    int64_t *urp;
+    int32_t *ucol, *uval = nullptr;
+    GK_CHECK(scr.alloc(&urp, m + 1));
+    GK_CHECK(scr.alloc(&ucol, low.nnz > 0 ? low.nnz : 1));
+    if (out_val && low.val) GK_CHECK(scr.alloc(&uval, low.nnz > 0 ? low.nnz : 1));
+    GK_CHECK(transpose_device(low, urp, ucol, uval, s, scr));
+    up.rp = urp;
+    up.col = ucol;
+    up.val = uval;
+    int64_t *crp;
+    int32_t *ccol, *cval = nullptr;
+    GK_CHECK(out_buffer(out_rowptr, static_cast<size_t>(m + 1), &crp, scr));
+    GK_CHECK(out_buffer(out_col, static_cast<size_t>(nnz), &ccol, scr));
+    if (out_val) GK_CHECK(out_buffer(out_val, static_cast<size_t>(nnz), &cval, scr));
+    k_add_rowptr<<<grid_for(m + 1), 256, 0, s>>>(m, low.rp, up.rp, crp);
+    note_launches(1);
+    GK_CUDA(cudaGetLastError());
+    int32_t *lrow, *urow;
+    GK_CHECK(entry_rows(low, &lrow, scr, s));
+    GK_CHECK(entry_rows(up, &urow, scr, s));
+    if (low.nnz > 0) {
+        k_add_place<<<grid_for(low.nnz), 256, 0, s>>>(low, lrow, up, 1, crp, ccol, cval);
+        k_add_place<<<grid_for(up.nnz), 256, 0, s>>>(up, urow, low, 0, crp, ccol, cval);
+        note_launches(2);
+    }
+    GK_CUDA(cudaGetLastError());
+    GK_CHECK(finish_out(out_rowptr, crp, static_cast<size_t>(m + 1), s));
+    GK_CHECK(finish_out(out_col, ccol, static_cast<size_t>(nnz), s));
+    if (out_val) GK_CHECK(finish_out(out_val, cval, static_cast<size_t>(nnz), s));
+    GK_CUDA(cudaStreamSynchronize(s));
+    return GK_OK;
+}
+
+static __global__ void k_fill_ones(int64_t n, int32_t *v) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) v[i] = 1;
+}
+
+// build_adjacency_matrix (include/matrix.h:643-660): G's pattern with every
+// value 1.
+extern "C" int gk_build_adjacency_matrix(const gk_csr *G, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
+                                         void *stream) {
+    GK_CHECK(validate_csr_shape(G, "G"));
+    const int64_t m = G->m, nnz = G->nnz;
+    if (!out_rowptr || (nnz > 0 && (!out_col || !out_val)))
+        return fail(GK_ERR_ARG, "build_adjacency_matrix: null output");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scr(s);
+    DevCsr g;
+    GK_CHECK(stage_csr(G, &g, scr, s, nullptr, CSR_STRUCTURE, "G"));
+    GK_CUDA(cudaMemcpyAsync(out_rowptr, g.rp, sizeof(int64_t) * (m + 1), cudaMemcpyDefault, s));
+    if (nnz > 0) {
+        GK_CUDA(cudaMemcpyAsync(out_col, g.col, sizeof(int32_t) * nnz, cudaMemcpyDefault, s));
+        int32_t *v;
+        GK_CHECK(out_buffer(out_val, static_cast<size_t>(nnz), &v, scr));
+        k_fill_ones<<<grid_for(nnz), 256, 0, s>>>(nnz, v);
+        note_launches(1);
+        GK_CUDA(cudaGetLastError());
+        GK_CHECK(finish_out(out_val, v, static_cast<size_t>(nnz), s));
+    }
+    GK_CUDA(cudaStreamSynchronize(s));
+    return GK_OK;
+}
+
 extern "C" int gk_dense_ewise_mult_masked(int64_t m, int64_t n, const double *A, const double *B, const gk_csr *M,
                                           double *C, void *stream) {
     GK_CHECK(check_dense_args(m, n, A, B, C));

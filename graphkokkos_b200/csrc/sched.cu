@@ -7,12 +7,14 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
 
 #include "gk_common.cuh"
+#include "gk_internal_host.h"
 #include "gk_sched.cuh"
 #include "gk_spgemm.cuh"
 
@@ -178,6 +180,42 @@ int sched_choose(const BinStats *bins, int *var_of_bin, int sched, int force_acc
 
 }  // namespace gk
 
+namespace gk {
+
+std::string read_model_file(const char *path, std::vector<float> &out) {
+    if (!path) return "path is null";
+    FILE *f = fopen(path, "rb");
+    if (!f) return std::string("cannot open ") + path;
+    unsigned char head[12];
+    std::string err;
+    if (fread(head, 1, sizeof(head), f) != sizeof(head) || memcmp(head, "GKMLP001", 8) != 0) {
+        err = std::string(path) + " is not a scheduler model file (magic GKMLP001)";
+    } else {
+        const uint32_t n = uint32_t(head[8]) | (uint32_t(head[9]) << 8) | (uint32_t(head[10]) << 16) |
+                           (uint32_t(head[11]) << 24);
+        if (n != static_cast<uint32_t>(MLP_SIZE)) {
+            err = std::string(path) + " holds " + std::to_string(n) + " weights, the model has " +
+                  std::to_string(MLP_SIZE);
+        } else {
+            std::vector<unsigned char> raw(4 * size_t(n) + 1);
+            if (fread(raw.data(), 1, raw.size(), f) != 4 * size_t(n)) {
+                err = std::string(path) + ": wrong length (truncated, or bytes after the weights)";
+            } else {
+                out.resize(n);
+                for (uint32_t i = 0; i < n; ++i) {
+                    const uint32_t b = uint32_t(raw[4 * i]) | (uint32_t(raw[4 * i + 1]) << 8) |
+                                       (uint32_t(raw[4 * i + 2]) << 16) | (uint32_t(raw[4 * i + 3]) << 24);
+                    memcpy(&out[i], &b, 4);
+                }
+            }
+        }
+    }
+    fclose(f);
+    return err;
+}
+
+}  // namespace gk
+
 extern "C" {
 
 int gk_sched_num_variants(void) { return gk::NV; }
@@ -201,6 +239,13 @@ int gk_sched_set_model(const float *weights, size_t n_floats) {
 int gk_sched_has_model(void) {
     std::lock_guard<std::mutex> lock(gk::g_model_mutex);
     return gk::g_model.empty() ? 0 : 1;
+}
+
+int gk_sched_load_model_file(const char *path) {
+    std::vector<float> w;
+    const std::string err = gk::read_model_file(path, w);
+    if (!err.empty()) return gk::fail(GK_ERR_ARG, "gk_sched_load_model_file: " + err);
+    return gk_sched_set_model(w.data(), w.size());
 }
 
 }  // extern "C"

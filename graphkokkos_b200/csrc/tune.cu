@@ -13,7 +13,6 @@ namespace gk {
 void bin_features_host(const BinStats &b, int epi, bool values, float *f);
 int plain_variant_host(int bin, const BinStats &b);
 
-int extract_lower_device(const DevCsr &A, int64_t *orp, int32_t *ocol, cudaStream_t s, Scratch &scr);
 
 // mode 0: triangle counting on L (A = B = M = L, sum of C);
 // mode 1: k-truss support on a symmetric A as gk_ktruss computes it

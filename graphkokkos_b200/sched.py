@@ -30,7 +30,9 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import math
 import os
+import re
 import time
 
 import numpy as np
@@ -61,22 +63,51 @@ def model_size():
 # ---------------------------------------------------------------------------
 # model I/O
 # ---------------------------------------------------------------------------
+MODEL_MAGIC = b"GKMLP001"
+
+
+def bin_path(npz_path):
+    """The model file (gk_sched_load_model_file layout) beside a .npz model."""
+    return os.path.splitext(npz_path)[0] + ".bin"
+
+
+def write_model_bin(w, path):
+    """Model file read by gk_sched_load_model_file / gk_bc_load_model_file:
+    magic, little-endian uint32 count, little-endian float32 weights."""
+    w = np.ascontiguousarray(w, dtype="<f4")
+    with open(path, "wb") as f:
+        f.write(MODEL_MAGIC + np.uint32(w.shape[0]).astype("<u4").tobytes() + w.tobytes())
+
+
+def read_model_bin(path):
+    raw = open(path, "rb").read()
+    if raw[:8] != MODEL_MAGIC:
+        raise ValueError(f"{path} is not a scheduler model file")
+    n = int(np.frombuffer(raw[8:12], dtype="<u4")[0])
+    return np.frombuffer(raw[12:12 + 4 * n], dtype="<f4").astype(np.float32)
+
+
 def load_model(path=MODEL_PATH):
-    w = np.ascontiguousarray(np.load(path)["w"], dtype=np.float32)
-    check(_lib.load().gk_sched_set_model(w.ctypes.data, w.shape[0]))
-    return w
+    """Loads the learned row-bin model through the library's file loader (the
+    call a C or C++ host makes); `path` may name the .npz or the .bin."""
+    path = bin_path(path)
+    check(_lib.load().gk_sched_load_model_file(path.encode()))
+    return read_model_bin(path)
 
 
 def load_bc_model(path=BC_MODEL_PATH):
-    """Loads the learned BC forward-shape model (gk_bc_set_model)."""
-    w = np.ascontiguousarray(np.load(path)["w"], dtype=np.float32)
-    check(_lib.load().gk_bc_set_model(w.ctypes.data, w.shape[0]))
-    return w
+    """Loads the learned BC forward-shape model (gk_bc_load_model_file)."""
+    path = bin_path(path)
+    check(_lib.load().gk_bc_load_model_file(path.encode()))
+    return read_model_bin(path)
 
 
 def save_model(w, path=MODEL_PATH, **meta):
+    """Writes the model as .npz (weights and training metadata) and as the
+    .bin model file the library loads."""
     os.makedirs(os.path.dirname(path), exist_ok=True)
     np.savez(path, w=np.asarray(w, dtype=np.float32), meta=json.dumps(meta))
+    write_model_bin(w, bin_path(path))
 
 
 # ---------------------------------------------------------------------------
@@ -253,7 +284,20 @@ def forward_numpy(w, X, nf, nv):
 # scheduler's margin follows GK_LEARNED_MARGIN as the library's does; the BC
 # level chooser's is fixed.
 BC_LEARNED_MARGIN = 0.1375
-LEARNED_MARGIN = float(os.environ.get("GK_LEARNED_MARGIN", BC_LEARNED_MARGIN))
+
+
+def _margin_from_env(text, default=BC_LEARNED_MARGIN):
+    """The library's parse of GK_LEARNED_MARGIN (csrc/sched.cu, learned_margin):
+    C atof (the longest leading decimal number, 0.0 when there is none), and
+    the default for an unset, non-finite or negative value."""
+    if text is None:
+        return default
+    mt = re.match(r"\s*([+-]?(?:inf(?:inity)?|nan|(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?))", text, re.IGNORECASE)
+    v = float(mt.group(1)) if mt else 0.0
+    return v if math.isfinite(v) and v >= 0.0 else default
+
+
+LEARNED_MARGIN = _margin_from_env(os.environ.get("GK_LEARNED_MARGIN"))
 
 
 def choose(out, recs):

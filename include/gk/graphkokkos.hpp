@@ -31,12 +31,26 @@
 //   * betweenness_centrality_batch(isParallel, A, b) keeps the reference's
 //     float return type and sources 0..b-1 but computes in FP64; the overload
 //     taking a source list returns the FP64 scores.
+//
+// Scheduler.  The reference picks its multiply by name (src/main.cpp:194-212);
+// here every call takes the process-wide schedule: the plain row-binning
+// heuristic by default, or the learned one after
+//   gk::use_learned_scheduler("graphkokkos_b200/sched/model.bin",
+//                             "graphkokkos_b200/sched/bc_model.bin");
+// or, without code changes, from the environment: GK_SCHED=learned with
+// GK_SCHED_MODEL and GK_BC_SCHED_MODEL naming the two model files (a model the
+// host already loaded with gk_sched_load_model_file / gk_bc_load_model_file
+// is used when the variable is unset).  The schedule changes which kernels
+// run, never the results.
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -48,6 +62,44 @@ namespace gkb_detail {
 
 inline void check(int status) {
     if (status != GK_OK) throw std::runtime_error(std::string("gk_b200: ") + gk_last_error_string());
+}
+
+// Process-wide schedule of the row-bin scheduler and of the BC level shapes.
+struct SchedChoice {
+    std::atomic<int> rows{GK_SCHED_PLAIN};
+    std::atomic<int> bc{GK_SCHED_PLAIN};
+    std::once_flag env;
+};
+inline SchedChoice &sched_choice() {
+    static SchedChoice c;
+    return c;
+}
+// GK_SCHED=learned: load the models named by GK_SCHED_MODEL / GK_BC_SCHED_MODEL
+// (or keep ones already loaded); a missing model is an error, not a silent
+// fallback to the plain schedule.
+inline void sched_from_env() {
+    std::call_once(sched_choice().env, [] {
+        const char *e = std::getenv("GK_SCHED");
+        if (!e || std::strcmp(e, "learned") != 0) return;
+        const char *rows = std::getenv("GK_SCHED_MODEL");
+        const char *bc = std::getenv("GK_BC_SCHED_MODEL");
+        if (rows) check(gk_sched_load_model_file(rows));
+        else if (!gk_sched_has_model())
+            throw std::runtime_error("gk_b200: GK_SCHED=learned needs GK_SCHED_MODEL (path of model.bin)");
+        if (bc) check(gk_bc_load_model_file(bc));
+        else if (!gk_bc_has_model())
+            throw std::runtime_error("gk_b200: GK_SCHED=learned needs GK_BC_SCHED_MODEL (path of bc_model.bin)");
+        sched_choice().rows = GK_SCHED_LEARNED;
+        sched_choice().bc = GK_SCHED_LEARNED;
+    });
+}
+inline int row_sched() {
+    sched_from_env();
+    return sched_choice().rows;
+}
+inline int bc_sched() {
+    sched_from_env();
+    return sched_choice().bc;
 }
 
 // Minimal shared 1-D array with the View call syntax used by the reference
@@ -80,6 +132,24 @@ private:
 };
 
 }  // namespace gkb_detail
+
+namespace gk {
+// Loads the learned scheduler's two models from their files and makes every
+// following call use them (throws std::runtime_error naming a bad file).
+inline void use_learned_scheduler(const char *model_path, const char *bc_model_path) {
+    gkb_detail::sched_from_env();
+    gkb_detail::check(gk_sched_load_model_file(model_path));
+    gkb_detail::check(gk_bc_load_model_file(bc_model_path));
+    gkb_detail::sched_choice().rows = GK_SCHED_LEARNED;
+    gkb_detail::sched_choice().bc = GK_SCHED_LEARNED;
+}
+// Back to the plain heuristic for every following call.
+inline void use_plain_scheduler() {
+    gkb_detail::sched_from_env();
+    gkb_detail::sched_choice().rows = GK_SCHED_PLAIN;
+    gkb_detail::sched_choice().bc = GK_SCHED_PLAIN;
+}
+}  // namespace gk
 
 template <typename ValT>
 class spMtx {
@@ -168,7 +238,7 @@ void mxmm_with(int accum, const spMtx<T> &A, const spMtx<T> &B, const spMtx<U> &
     gk_csr a = A.csr(), b = B.csr();
     gk_csr mm{static_cast<int64_t>(M.m), static_cast<int64_t>(M.n), static_cast<int64_t>(M.nz), M.Rst.data(),
               M.Col.data(), nullptr};
-    check(gk_mxmm_masked(&a, &b, &mm, R.Val.data(), GK_PLUS_TIMES, GK_SCHED_PLAIN, accum, nullptr));
+    check(gk_mxmm_masked(&a, &b, &mm, R.Val.data(), GK_PLUS_TIMES, row_sched(), accum, nullptr));
     C = R;
 }
 }  // namespace gkb_detail
@@ -187,7 +257,7 @@ template <typename T>
 void mxmm_naive(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, spMtx<T> &C) {
     gkb_detail::mxmm_with(GK_ACCUM_HASH, A, B, M, C);
 }
-// Scheduler's choice per row bin (plain heuristic).
+// Scheduler's choice per row bin (plain heuristic or learned model, see the top).
 template <typename T>
 void mxmm_gpu(bool, const spMtx<T> &A, const spMtx<T> &B, const spMtx<T> &M, spMtx<T> &C) {
     gkb_detail::mxmm_with(GK_ACCUM_AUTO, A, B, M, C);
@@ -281,32 +351,22 @@ spMtx<T> extract_lower_triangle(const spMtx<T> &A) {
     return R;
 }
 
+// Both run on the GPU (gk_build_symm_from_lower, gk_build_adjacency_matrix).
 template <typename T>
 spMtx<T> build_symm_from_lower(const spMtx<T> &Low) {
-    spMtx<T> U = transpose(Low);
+    static_assert(std::is_same<T, int>::value, "the GPU transforms take int matrices (spMtx<int>)");
     spMtx<T> R(Low.m, Low.n, 2 * Low.nz);
-    size_t jr = 0;
-    for (size_t i = 0; i < Low.m; ++i) {
-        int64_t jl = Low.Rst(i), xl = Low.Rst(i + 1), ju = U.Rst(i), xu = U.Rst(i + 1);
-        while (jl < xl && ju < xu) {
-            if (Low.Col(jl) < U.Col(ju)) { R.Col(jr) = Low.Col(jl); R.Val(jr++) = Low.Val(jl++); }
-            else { R.Col(jr) = U.Col(ju); R.Val(jr++) = U.Val(ju++); }
-        }
-        while (jl < xl) { R.Col(jr) = Low.Col(jl); R.Val(jr++) = Low.Val(jl++); }
-        while (ju < xu) { R.Col(jr) = U.Col(ju); R.Val(jr++) = U.Val(ju++); }
-        R.Rst(i + 1) = static_cast<int64_t>(jr);
-    }
+    gk_csr l = Low.csr();
+    gkb_detail::check(gk_build_symm_from_lower(&l, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
     return R;
 }
 
 template <typename T>
 spMtx<int> build_adjacency_matrix(const spMtx<T> &G) {
     spMtx<int> R(G.m, G.n, G.nz);
-    std::copy(G.Rst.data(), G.Rst.data() + G.m + 1, R.Rst.data());
-    for (size_t j = 0; j < G.nz; ++j) {
-        R.Col(j) = G.Col(j);
-        R.Val(j) = 1;
-    }
+    gk_csr g{static_cast<int64_t>(G.m), static_cast<int64_t>(G.n), static_cast<int64_t>(G.nz), G.Rst.data(),
+             G.Col.data(), nullptr};
+    gkb_detail::check(gk_build_adjacency_matrix(&g, R.Rst.data(), R.Col.data(), R.Val.data(), nullptr));
     return R;
 }
 
@@ -323,7 +383,7 @@ inline int64_t triangle_counting_masked_sandia(const spMtx<int> &A, mxmOp<int> m
     if (ours) {
         gk_csr l = L.csr(false);
         uint64_t count = 0;
-        gkb_detail::check(gk_tc_count(&l, &count, GK_SCHED_PLAIN, nullptr));
+        gkb_detail::check(gk_tc_count(&l, &count, gkb_detail::row_sched(), nullptr));
         return static_cast<int64_t>(count);
     }
     spMtx<int> C;
@@ -345,7 +405,7 @@ inline int *triangle_counting_vertex(const spMtx<int> &A, mxmOp<int> matrixMult,
     if (ours) {
         gk_csr a = A.csr(false);
         try {
-            gkb_detail::check(gk_tc_vertex(&a, reinterpret_cast<int32_t *>(nums), GK_SCHED_PLAIN, nullptr));
+            gkb_detail::check(gk_tc_vertex(&a, reinterpret_cast<int32_t *>(nums), gkb_detail::row_sched(), nullptr));
         } catch (...) {
             delete[] nums;
             throw;
@@ -371,7 +431,7 @@ inline int64_t triangle_counting_masked_lu(const spMtx<int> &A, mxmOp<int> matri
     if (ours) {
         gk_csr a = A.csr(false);
         uint64_t count = 0;
-        gkb_detail::check(gk_tc_count_lu(&a, &count, GK_SCHED_PLAIN, nullptr));
+        gkb_detail::check(gk_tc_count_lu(&a, &count, gkb_detail::row_sched(), nullptr));
         return static_cast<int64_t>(count);
     }
     spMtx<int> L = extract_lower_triangle(A);
@@ -392,7 +452,7 @@ inline spMtx<int> k_truss(const spMtx<int> &A, int k, mxmOp<int>, bool, int *ite
     gk_csr_mut io{static_cast<int64_t>(A.m), static_cast<int64_t>(A.n), static_cast<int64_t>(A.nz), C.Rst.data(),
                   C.Col.data()};
     int iters = 0;
-    gkb_detail::check(gk_ktruss(&io, k, &iters, GK_SCHED_PLAIN, nullptr));
+    gkb_detail::check(gk_ktruss(&io, k, &iters, gkb_detail::row_sched(), nullptr));
     C.resizeVals(static_cast<size_t>(io.nnz));
     for (size_t j = 0; j < C.nz; ++j) C.Val(j) = 1;
     if (iterations) *iterations = iters;
@@ -408,14 +468,14 @@ inline std::vector<float> betweenness_centrality_batch(bool, const spMtx<int> &A
     for (size_t j = 0; j < b; ++j) src[j] = static_cast<int32_t>(j);
     std::vector<double> d(A.m);
     gk_csr a = A.csr();
-    gkb_detail::check(gk_bc_batch(&a, src.data(), static_cast<int>(b), d.data(), GK_SCHED_PLAIN, nullptr));
+    gkb_detail::check(gk_bc_batch(&a, src.data(), static_cast<int>(b), d.data(), gkb_detail::bc_sched(), nullptr));
     return std::vector<float>(d.begin(), d.end());
 }
 
 inline std::vector<double> betweenness_centrality_batch(const spMtx<int> &A, const std::vector<int32_t> &sources) {
     std::vector<double> d(A.m);
     gk_csr a = A.csr();
-    gkb_detail::check(gk_bc_batch(&a, sources.data(), static_cast<int>(sources.size()), d.data(), GK_SCHED_PLAIN,
-                                  nullptr));
+    gkb_detail::check(gk_bc_batch(&a, sources.data(), static_cast<int>(sources.size()), d.data(),
+                                  gkb_detail::bc_sched(), nullptr));
     return d;
 }

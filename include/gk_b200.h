@@ -222,6 +222,19 @@ int gk_extract_lower(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int
 int gk_transpose(const gk_csr *A, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
                  void *stream);
 
+/* Symmetric matrix from its strict lower triangle (build_symm_from_lower,
+ * include/matrix.h:662-696): row i of the result merges row i of L with row i
+ * of transpose(L), the transpose's entry first on equal columns, values
+ * carried (out_val may be NULL; L's NULL values count as 1).  L must be square
+ * with sorted rows.  out_rowptr: m+1, out_col / out_val: 2*nnz(L). */
+int gk_build_symm_from_lower(const gk_csr *L, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
+                             void *stream);
+
+/* G's pattern with every value 1 (build_adjacency_matrix,
+ * include/matrix.h:643-660).  out_rowptr: m+1, out_col / out_val: nnz. */
+int gk_build_adjacency_matrix(const gk_csr *G, int64_t *out_rowptr, int32_t *out_col, int32_t *out_val,
+                              void *stream);
+
 /* ----- graph generation (device-side builder; host twin: gk_gen_*_host) ------- */
 
 /* Seeded RMAT graph (2^scale vertices, edge_factor << scale edges) or
@@ -282,6 +295,16 @@ size_t gk_sched_model_size(void);
 int gk_sched_set_model(const float *weights, size_t n_floats);
 int gk_sched_has_model(void);
 
+/* Loads the learned scheduler's MLP from a model file, so that a C or C++ host
+ * can use GK_SCHED_LEARNED without parsing anything itself.  File layout: the
+ * 8 bytes "GKMLP001", a little-endian uint32 weight count (gk_sched_model_size()),
+ * then the float32 weights little-endian.  The trained models ship as
+ * graphkokkos_b200/sched/model.bin (row bins) and bc_model.bin (BC levels).
+ * GK_ERR_ARG names what is wrong with a file that does not match.  No
+ * counterpart in the reference, whose only schedule choice is the CLI's
+ * accumulator name (src/main.cpp:194-212). */
+int gk_sched_load_model_file(const char *path);
+
 /* ----- autotuning and training of the learned scheduler (no reference
  * counterpart: the reference's only scheduling is the CLI's per-call accumulator
  * choice, src/main.cpp:194-212) ------------------------------------------------ */
@@ -329,6 +352,8 @@ int gk_mlp_forward(const float *w, const float *X, int n, float *out, void *stre
  * in FP64, exact in any order of addition. */
 int gk_bc_set_model(const float *weights, size_t n_floats);
 int gk_bc_has_model(void);
+/* Same from a model file (layout of gk_sched_load_model_file). */
+int gk_bc_load_model_file(const char *path);
 
 /* Autotuning run of gk_bc_batch (at most 512 sources, one chunk) with every
  * forward level on `shape` (0 pull, 1 push, -1 the plain rule), the levels

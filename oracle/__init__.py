@@ -15,6 +15,13 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# The reference checkout whose sources the reference oracle compiles in place:
+# GK_REFERENCE_DIR, else the checkout's location on the build host.
+REFERENCE_DIR = os.environ.get("GK_REFERENCE_DIR", "/root/reference")
+
+
+def reference_present():
+    return os.path.isdir(os.path.join(REFERENCE_DIR, "include"))
 PORT_PATH = os.path.join(HERE, "_build", "libgk_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libgk_ref.so")
 
@@ -22,11 +29,13 @@ _port = None
 _ref = None
 
 
-def build(ref=True):
-    """Builds the port (always) and the reference oracle (when the reference
-    sources are present)."""
-    targets = ["port", "ref"] if ref else ["port"]
-    out = subprocess.run(["make", "-C", HERE] + targets, capture_output=True, text=True)
+def build(ref=True, adapter=False):
+    """Builds the port (always), the reference oracle (when the reference
+    sources are present) and, with adapter=True, the reference-side adapter
+    of the integration guide (needs libgk_b200.so built first)."""
+    targets = ["port"] + (["ref"] if ref else []) + (["adapter"] if adapter else [])
+    env = dict(os.environ, GK_REFERENCE_DIR=REFERENCE_DIR if reference_present() else "")
+    out = subprocess.run(["make", "-C", HERE] + targets, capture_output=True, text=True, env=env)
     if out.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{out.stdout}\n{out.stderr}")
 
@@ -462,3 +471,55 @@ def relabel_sources_first(A, sources):
     c.m = c.n = m
     c.rowptr, c.col, c.val = nrp, nc.astype(np.int32), None
     return c, perm
+
+
+# ----- synthetic inputs (independent of the product library) ---------------------
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+class HostCsr:
+    """A host CSR (numpy arrays), the fields the oracle functions read."""
+
+    def __init__(self, m, rowptr, col):
+        self.m = self.n = m
+        self.rowptr = rowptr
+        self.col = col
+        self.val = None
+        self.nnz = int(len(col))
+
+
+def _take_graph(h, lower):
+    lib = port()
+    m, nnz = ctypes.c_int64(0), ctypes.c_int64(0)
+    lib.orc_graph_info(h, ctypes.byref(m), ctypes.byref(nnz))
+    rp = np.zeros(m.value + 1, dtype=np.int64)
+    col = np.zeros(max(nnz.value, 1), dtype=np.int32)
+    got = lib.orc_graph_copy(h, ctypes.c_int(1 if lower else 0), _p(rp), _p(col))
+    lib.orc_graph_free(h)
+    return HostCsr(m.value, rp, col[:got].copy())
+
+
+def _gen_lib():
+    lib = port()
+    lib.orc_gen_rmat.restype = ctypes.c_void_p
+    lib.orc_gen_rmat.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_uint64]
+    lib.orc_gen_er.restype = ctypes.c_void_p
+    lib.orc_gen_er.argtypes = [I64, I64, ctypes.c_uint64]
+    lib.orc_graph_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.orc_graph_copy.restype = I64
+    lib.orc_graph_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    lib.orc_graph_free.argtypes = [ctypes.c_void_p]
+    return lib
+
+
+def gen_rmat(scale, edge_factor=16, seed=1, lower=False, abc=RMAT_ABC):
+    """Seeded RMAT graph (symmetric, or its strict lower triangle) from the
+    oracle's own restatement of the generator."""
+    h = _gen_lib().orc_gen_rmat(scale, edge_factor, abc[0], abc[1], abc[2], seed)
+    return _take_graph(h, lower)
+
+
+def gen_er(n, nedges, seed=1, lower=False):
+    h = _gen_lib().orc_gen_er(n, nedges, seed)
+    return _take_graph(h, lower)

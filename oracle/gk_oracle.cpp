@@ -416,6 +416,10 @@ int orc_mlp_loss_grad(int F, int H, int V, const float *w, const float *X, const
 //             Bcu<S_{d-1}> += (A·W)∘Numsp,   Bcu starts at 1 (:476-478)
 //   result   (:490-497): bc[v] = sum_j Bcu(v,j) - b.
 // Values of A are used as the reference uses them (a_val factors).
+// Bcu(v,j) = 1 + delta(v,j), with delta assigned once (when v's level is
+// processed); the result is accumulated as sum_j delta(v,j), which equals
+// sum_j (Bcu(v,j) - 1) in exact arithmetic and keeps the full FP64 precision
+// of a small delta that 1 + delta - 1 would round away.
 // ---------------------------------------------------------------------------
 int orc_bc_f64(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *val,
                const int32_t *src, int64_t b, double *bc_out) {
@@ -430,7 +434,7 @@ int orc_bc_f64(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *
     {
         const int tid = omp_get_thread_num();
         double *mine = acc_total.data() + static_cast<size_t>(m) * tid;
-        std::vector<double> numsp(m), bcu(m), frontv(m), nextv(m);
+        std::vector<double> numsp(m), bcu(m), dlt(m), frontv(m), nextv(m);
         std::vector<int32_t> depth(m);
         std::vector<int32_t> front, next;
         std::vector<std::vector<int32_t>> levels;
@@ -488,7 +492,10 @@ int orc_bc_f64(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *
                 ++d;
             }
             // backward (:469-488); Sigmas values are the frontier's path counts
-            for (int64_t v = 0; v < m; ++v) bcu[v] = 1.0;
+            for (int64_t v = 0; v < m; ++v) {
+                bcu[v] = 1.0;
+                dlt[v] = 0.0;
+            }
             const int D = static_cast<int>(levels.size());
             for (int lk = D - 1; lk > 0; --lk) {
                 // W = Nspinv ∘ Bcu on the pattern of Sigmas[lk] (:192-199)
@@ -499,11 +506,12 @@ int orc_bc_f64(int64_t m, const int64_t *rp, const int32_t *col, const int32_t *
                         const int32_t w = col[t];
                         if (depth[w] == lk + 1) sum += static_cast<double>(val ? val[t] : 1) * frontv[w];
                     }
-                    bcu[v] += sum * numsp[v];  // (:236-239)
+                    dlt[v] = sum * numsp[v];  // (:236-239): Bcu += (A·W)∘Numsp
+                    bcu[v] = 1.0 + dlt[v];
                 }
                 for (int32_t w : levels[lk]) frontv[w] = 0.0;
             }
-            for (int64_t v = 0; v < m; ++v) mine[v] += bcu[v] - 1.0;
+            for (int64_t v = 0; v < m; ++v) mine[v] += dlt[v];
         }
     }
     const int nt = omp_get_max_threads();
@@ -578,5 +586,146 @@ int orc_mxmm_spd(int64_t m, const int64_t *arp, const int32_t *acol, const doubl
         }
     return 0;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Synthetic inputs for the CPU side of the benchmark (the reference arm and
+// the CPU baseline), restated independently of the library's builder so that
+// timing the reference never loads the product library.  Same definition as
+// the library's generator: every draw is splitmix64's output function
+// (Steele, Lea & Flood, OOPSLA 2014) of key ^ counter with
+// key = mix(seed ^ 0x6A09E667F3BCC909); RMAT edge e (Chakrabarti, Zhan &
+// Faloutsos, SDM 2004) takes one quadrant per level, most significant bit
+// first, from the high 32 bits of draw mix(key ^ (e << 6 | level)) against
+// integer thresholds a, a+b, a+b+c of 2^32; Erdos-Renyi pair e is
+// (hi32 * n >> 32, lo32 * n >> 32) of draw mix(key ^ (e << 1)).  The edge
+// list is symmetrised, self-loops and duplicates dropped, rows sorted.
+// tests/test_oracle.py checks it equals the library's builder bit for bit.
+// ---------------------------------------------------------------------------
+namespace {
+inline uint64_t splitmix_out(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+uint32_t threshold(double p) {
+    const double s = 4294967296.0;
+    const double x = p * s;
+    return x >= s ? 0xFFFFFFFFu : static_cast<uint32_t>(x);
+}
+
+struct GenGraph {
+    int64_t m = 0;
+    std::vector<int64_t> rp;
+    std::vector<int32_t> col;
+};
+
+// Symmetric CSR from an edge list (u[e], v[e]): a degree count, a scatter of
+// both directions per row, then each row sorted and de-duplicated in parallel.
+void symmetric_csr(int64_t n, const std::vector<uint32_t> &u, const std::vector<uint32_t> &v, GenGraph &g) {
+    const int64_t ne = static_cast<int64_t>(u.size());
+    std::vector<int64_t> cnt(n + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < ne; ++e) {
+        if (u[e] == v[e]) continue;
+#pragma omp atomic
+        cnt[u[e] + 1]++;
+#pragma omp atomic
+        cnt[v[e] + 1]++;
+    }
+    for (int64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int32_t> buf(cnt[n]);
+    std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < ne; ++e) {
+        if (u[e] == v[e]) continue;
+        int64_t p, q;
+#pragma omp atomic capture
+        p = cur[u[e]]++;
+#pragma omp atomic capture
+        q = cur[v[e]]++;
+        buf[p] = static_cast<int32_t>(v[e]);
+        buf[q] = static_cast<int32_t>(u[e]);
+    }
+    std::vector<int64_t> len(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t *b = buf.data() + cnt[i], *e = buf.data() + cnt[i + 1];
+        std::sort(b, e);
+        len[i] = std::unique(b, e) - b;
+    }
+    g.m = n;
+    g.rp.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) g.rp[i + 1] = g.rp[i] + len[i];
+    g.col.resize(g.rp[n]);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; ++i) std::copy(buf.data() + cnt[i], buf.data() + cnt[i] + len[i], g.col.data() + g.rp[i]);
+}
+}  // namespace
+
+extern "C" {
+
+// RMAT graph with 2^scale vertices and ef * 2^scale generated edges; returns
+// an opaque handle (orc_graph_info / orc_graph_copy / orc_graph_free).
+void *orc_gen_rmat(int scale, int ef, double a, double b, double c, uint64_t seed) {
+    const uint64_t key = splitmix_out(seed ^ 0x6A09E667F3BCC909ull);
+    const uint32_t ta = threshold(a), tab = threshold(a + b), tabc = threshold(a + b + c);
+    const int64_t n = int64_t(1) << scale, ne = static_cast<int64_t>(ef) << scale;
+    std::vector<uint32_t> u(ne), v(ne);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < ne; ++e) {
+        uint32_t uu = 0, vv = 0;
+        for (int l = 0; l < scale; ++l) {
+            const uint32_t r = static_cast<uint32_t>(splitmix_out(key ^ ((static_cast<uint64_t>(e) << 6) | l)) >> 32);
+            uu = (uu << 1) | (r >= tab ? 1u : 0u);
+            vv = (vv << 1) | (((r >= ta && r < tab) || r >= tabc) ? 1u : 0u);
+        }
+        u[e] = uu;
+        v[e] = vv;
+    }
+    GenGraph *g = new GenGraph;
+    symmetric_csr(n, u, v, *g);
+    return g;
+}
+
+// Erdos-Renyi G(n, M) with M = nedges generated pairs.
+void *orc_gen_er(int64_t n, int64_t nedges, uint64_t seed) {
+    const uint64_t key = splitmix_out(seed ^ 0x6A09E667F3BCC909ull);
+    std::vector<uint32_t> u(nedges), v(nedges);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < nedges; ++e) {
+        const uint64_t h = splitmix_out(key ^ (static_cast<uint64_t>(e) << 1));
+        u[e] = static_cast<uint32_t>(((h >> 32) * static_cast<uint64_t>(n)) >> 32);
+        v[e] = static_cast<uint32_t>(((h & 0xFFFFFFFFull) * static_cast<uint64_t>(n)) >> 32);
+    }
+    GenGraph *g = new GenGraph;
+    symmetric_csr(n, u, v, *g);
+    return g;
+}
+
+void orc_graph_info(void *h, int64_t *m, int64_t *nnz) {
+    const GenGraph *g = static_cast<GenGraph *>(h);
+    *m = g->m;
+    *nnz = g->rp[g->m];
+}
+
+// Copies the symmetric graph (lower = 0) or its strict lower triangle
+// (lower = 1: rp gets m+1 entries, col the lower entries); col must hold
+// the symmetric graph's nnz entries.  Returns the number of entries copied.
+int64_t orc_graph_copy(void *h, int lower, int64_t *rp, int32_t *col) {
+    const GenGraph *g = static_cast<GenGraph *>(h);
+    if (!lower) {
+        std::copy(g->rp.begin(), g->rp.end(), rp);
+        std::copy(g->col.begin(), g->col.end(), col);
+        return g->rp[g->m];
+    }
+    int64_t nz = 0;
+    return orc_extract_lower(g->m, g->rp.data(), g->col.data(), rp, col, &nz) == 0 ? nz : -1;
+}
+
+void orc_graph_free(void *h) { delete static_cast<GenGraph *>(h); }
 
 }  // extern "C"

@@ -26,11 +26,16 @@
 //   * TeamPolicy runs one team per OpenMP thread with team size 1 and a
 //     dynamic schedule over league ranks (Kokkos' OpenMP backend with
 //     Kokkos::AUTO resolves to this on a host build).
+//   * Per-thread scratch comes from a pool that each OpenMP thread keeps
+//     between kernels (grown on demand, never shrunk), as Kokkos' scratch pool.
 // Two documented deviations from Kokkos, both needed for the reference code
 // to run as its author intended:
-//   * Per-thread scratch is ZERO-FILLED for every team
+//   * Per-thread scratch is ZERO-FILLED for every team by default
 //     (betweenness_centrality.h:347-363 and :379-397 read scratch before
-//     writing it; real Kokkos leaves scratch uninitialised).
+//     writing it; real Kokkos leaves scratch uninitialised).  A caller that
+//     times code which does not rely on it (the MSA product clears its
+//     accumulator at the mask columns, matrix_la.h:614-616) turns the fill off
+//     for a scope with kokkos_shim::ScratchZeroFill.
 //   * deep_copy() between rank-1 views of different extents copies the common
 //     prefix instead of aborting.  The reference k-truss loop
 //     (main.cpp:106-130) passes a matrix whose Col extent is larger than its
@@ -51,6 +56,29 @@
 #define KOKKOS_LAMBDA [=]
 #define KOKKOS_INLINE_FUNCTION inline
 #define KOKKOS_FUNCTION
+
+namespace kokkos_shim {
+// The calling OpenMP thread's scratch pool, at least `bytes` long.
+inline char *thread_scratch(size_t bytes) {
+    static thread_local std::vector<char> pool;
+    if (pool.size() < bytes) {
+        pool.clear();
+        pool.shrink_to_fit();
+        pool.resize(bytes);
+    }
+    return pool.data();
+}
+inline bool &zero_scratch_flag() {
+    static bool zero = true;
+    return zero;
+}
+// Scope in which TeamPolicy scratch is (or is not) zero-filled per team.
+struct ScratchZeroFill {
+    bool saved;
+    explicit ScratchZeroFill(bool on) : saved(zero_scratch_flag()) { zero_scratch_flag() = on; }
+    ~ScratchZeroFill() { zero_scratch_flag() = saved; }
+};
+}  // namespace kokkos_shim
 
 namespace Kokkos {
 
@@ -281,13 +309,14 @@ template <class F, class... A>
 void parallel_for(const std::string &, const TeamPolicy<A...> &p, const F &f) {
     const size_t bytes = p.scratch_bytes;
     const int64_t league = p.league_size;
+    const bool zero = kokkos_shim::zero_scratch_flag();
 #pragma omp parallel
     {
-        std::vector<char> arena(bytes > 0 ? bytes : 8);
+        char *arena = kokkos_shim::thread_scratch(bytes > 0 ? bytes : 8);
 #pragma omp for schedule(dynamic, 1)
         for (int64_t r = 0; r < league; ++r) {
-            std::memset(arena.data(), 0, arena.size());
-            ScratchMemorySpace space{arena.data(), bytes, 0};
+            if (zero) std::memset(arena, 0, bytes);
+            ScratchMemorySpace space{arena, bytes, 0};
             TeamMember member(static_cast<int>(r), static_cast<int>(league), &space);
             f(member);
         }

@@ -39,9 +39,40 @@ spMtx<int> make_mtx(int64_t m, int64_t n, const int64_t *rp, const int32_t *col,
     return A;
 }
 
+// The reference's parallel MSA (matrix_la.h:590-595) splits rows over
+// T = Kokkos::num_threads() teams with `if (A.Rst[i] >= A.nz * team_i / T)
+// work_distribution(team_i++) = i` over every i <= m.  When A.nz < T the
+// threshold A.nz * (T + 1) / T equals A.nz, so each trailing row with
+// Rst == nz writes one more entry past the T + 1 the View holds (and with
+// A.nz == 0 every row does): a heap overflow.  A.nz >= T keeps every write in
+// bounds, so this wrapper runs the reference with min(T, A.nz) threads, and
+// for an operand without entries returns what the reference defines without
+// calling it: C with M's pattern (matrix_la.h:564-568) and zero values.
+struct ThreadCap {
+    int saved;
+    explicit ThreadCap(int64_t nz) : saved(omp_get_max_threads()) {
+        if (nz < saved) omp_set_num_threads(static_cast<int>(nz > 0 ? nz : 1));
+    }
+    ~ThreadCap() { omp_set_num_threads(saved); }
+};
+
+void msa_guarded(bool isParallel, const spMtx<int> &A, const spMtx<int> &B, const spMtx<int> &M, spMtx<int> &C) {
+    if (A.nz == 0) {
+        C.resizeRows(M.m);
+        C.resizeVals(M.nz);
+        C.n = M.n;
+        Kokkos::deep_copy(C.Col, M.Col);
+        Kokkos::deep_copy(C.Rst, M.Rst);
+        for (size_t j = 0; j < M.nz; ++j) C.Val(j) = 0;
+        return;
+    }
+    ThreadCap cap(static_cast<int64_t>(A.nz));
+    mxmm_msa<int, int>(isParallel, A, B, M, C);
+}
+
 mxmOp<int> pick(int accum) {
     switch (accum) {
-        case 0: return mxmm_msa<int, int>;
+        case 0: return msa_guarded;
         case 1: return mxmm_mca<int, int>;
         case 2: return mxmm_naive<int>;
         default: return nullptr;
@@ -338,7 +369,7 @@ int ref_tc_rows(int parallel, int64_t m, const int64_t *rp, const int32_t *col,
             S.Val(j - rp[row_begin]) = 1;
         }
         spMtx<int> C;
-        mxmm_msa(parallel != 0, S, L, S, C);
+        msa_guarded(parallel != 0, S, L, S, C);
         int64_t num_of_tr = 0;
         Kokkos::parallel_reduce("", C.nz, KOKKOS_LAMBDA(int64_t i, int64_t &sum) { sum += C.Val(i); },
                                 Kokkos::Sum<int64_t>(num_of_tr));
@@ -349,35 +380,46 @@ int ref_tc_rows(int parallel, int64_t m, const int64_t *rp, const int32_t *col,
     }
 }
 
-// Bounded sample for CPU timing: C<S> = S·L with S = the rows i of L with
-// i % stride == offset (other rows empty), through the reference mxmm_msa.
-// Returns the sum of C (the sampled rows' share of the triangle count) and the
-// number of sampled L entries.  `seconds` receives the time spent inside
-// mxmm_msa plus the sum, the reference's own bracket (src/main.cpp:74-85).
+// Bounded sample for CPU timing: C<S> = S·L through the reference mxmm_msa,
+// with S = the rows i of L with i % stride == offset, compacted to a matrix of
+// those rows only (r rows, m columns): the reference's per-call costs that
+// scale with the row count (the copy of M's pattern into C, matrix_la.h:564-568,
+// and the serial work split, :590-596) then follow the sample, not the whole
+// graph, so the measured rate is the rate of the reference's row loop.  The
+// shim's per-thread scratch is kept between calls and not zero-filled here, as
+// Kokkos' own scratch pool is (the MSA clears its accumulator at the mask
+// columns before each row, :614-616).  Returns the sum of C (the sampled rows'
+// share of the triangle count) and the number of sampled L entries; `seconds`
+// receives the time inside mxmm_msa plus the sum, the reference's own bracket
+// (src/main.cpp:74-85).
 int ref_tc_row_stride(int64_t m, const int64_t *rp, const int32_t *col, int64_t stride, int64_t offset,
                       int64_t *out, int64_t *sample_nnz, double *seconds) {
     try {
         spMtx<int> L = make_mtx(m, m, rp, col, nullptr);
-        int64_t nz = 0;
-        for (int64_t i = offset; i < m; i += stride) nz += rp[i + 1] - rp[i];
-        if (nz == 0) {  // the reference's mxmm_msa corrupts the heap on an empty operand
+        int64_t nz = 0, r = 0;
+        for (int64_t i = offset; i < m; i += stride) {
+            nz += rp[i + 1] - rp[i];
+            ++r;
+        }
+        if (nz == 0) {  // no entries: the sample's count is 0 (see msa_guarded)
             *out = 0;
             *sample_nnz = 0;
             *seconds = 0.0;
             return 0;
         }
-        spMtx<int> S(static_cast<size_t>(m), static_cast<size_t>(m), static_cast<size_t>(nz));
-        int64_t pos = 0;
+        spMtx<int> S(static_cast<size_t>(r), static_cast<size_t>(m), static_cast<size_t>(nz));
+        int64_t pos = 0, row = 0;
         S.Rst(0) = 0;
-        for (int64_t i = 0; i < m; ++i) {
-            if (i % stride == offset)
-                for (int64_t j = rp[i]; j < rp[i + 1]; ++j) {
-                    S.Col(pos) = col[j];
-                    S.Val(pos++) = 1;
-                }
-            S.Rst(i + 1) = static_cast<int>(pos);
+        for (int64_t i = offset; i < m; i += stride) {
+            for (int64_t j = rp[i]; j < rp[i + 1]; ++j) {
+                S.Col(pos) = col[j];
+                S.Val(pos++) = 1;
+            }
+            S.Rst(++row) = static_cast<int>(pos);
         }
         spMtx<int> C;
+        ThreadCap cap(nz);
+        kokkos_shim::ScratchZeroFill keep_scratch(false);
         auto t0 = std::chrono::steady_clock::now();
         mxmm_msa(true, S, L, S, C);
         int64_t num_of_tr = 0;

@@ -109,3 +109,23 @@ def brandes_f64(csr, sources):
             if v != s:
                 bc[v] += delta[v]
     return bc
+
+
+def bc_mismatches(got, want, rtol=1e-12):
+    """Vertices whose FP64 BC score is not within rtol relative of the oracle's;
+    an oracle score of exactly 0 must be exactly 0 (no absolute tolerance)."""
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    assert got.shape == want.shape, (got.shape, want.shape)
+    zero = want == 0.0
+    bad = np.where(zero, got != 0.0, ~(np.abs(got - want) <= rtol * np.abs(want)))
+    return np.flatnonzero(bad)
+
+
+def assert_bc_close(got, want, rtol=1e-12):
+    bad = bc_mismatches(got, want, rtol)
+    if len(bad):
+        got = np.asarray(got, dtype=np.float64)
+        want = np.asarray(want, dtype=np.float64)
+        show = ", ".join(f"v{v}: {got[v]!r} vs {want[v]!r}" for v in bad[:5])
+        raise AssertionError(f"{len(bad)} of {len(want)} BC scores outside rtol {rtol} (atol 0): {show}")

@@ -49,6 +49,30 @@ def test_bad_model_rejected(gk):
     assert b"gk_sched_model_size" in lib.gk_last_error_string()
 
 
+def test_model_files_load_from_c(gk, tmp_path):
+    """The shipped model files load through the C entry points a C/C++ host
+    calls (host code only), equal the training output (.npz), and malformed
+    files are refused with a reason."""
+    from graphkokkos_b200 import sched
+    lib = gk.load()
+    for npz, loader in ((sched.MODEL_PATH, lib.gk_sched_load_model_file),
+                        (sched.BC_MODEL_PATH, lib.gk_bc_load_model_file)):
+        path = sched.bin_path(npz)
+        assert loader(path.encode()) == 0, lib.gk_last_error_string()
+        np.testing.assert_array_equal(sched.read_model_bin(path), np.load(npz)["w"].astype(np.float32))
+        raw = open(path, "rb").read()
+        for name, data, why in (("short", raw[:-4], b"wrong length"), ("long", raw + b"\0\0\0\0", b"wrong length"),
+                                ("magic", b"XXXXXXXX" + raw[8:], b"GKMLP001"),
+                                ("count", raw[:8] + b"\x05\0\0\0" + raw[12:], b"holds 5 weights")):
+            bad = tmp_path / name
+            bad.write_bytes(data)
+            assert loader(str(bad).encode()) == 1, name
+            assert why in lib.gk_last_error_string(), (name, lib.gk_last_error_string())
+        assert loader(str(tmp_path / "absent.bin").encode()) == 1
+        assert b"cannot open" in lib.gk_last_error_string()
+    assert lib.gk_sched_has_model() == 1 and lib.gk_bc_has_model() == 1
+
+
 def test_missing_library_fails_loudly(monkeypatch):
     import graphkokkos_b200._lib as L
     monkeypatch.setattr(L, "_lib", None)

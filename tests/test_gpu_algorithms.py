@@ -113,18 +113,18 @@ def test_bc_matches_oracle(gk, orc, cuda, scale, nsrc, seed):
     src = rng.choice(A.m, size=nsrc, replace=False)
     want = orc.bc_f64(A, src)
     got = gk.bc_batch(dev(A), src).cpu().numpy()
-    np.testing.assert_allclose(got, want, rtol=BC_RTOL, atol=1e-9)
+    G.assert_bc_close(got, want, BC_RTOL)
 
 
 def test_bc_more_than_one_chunk(gk, orc, cuda):
     A = gk.gen_rmat(10, 8, seed=9)
     src = np.random.default_rng(1).choice(A.m, size=700, replace=False)
-    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), rtol=BC_RTOL, atol=1e-9)
+    G.assert_bc_close(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), BC_RTOL)
 
 
 def test_bc_closed_forms_and_host_buffers(gk, cuda):
     bc = gk.bc_batch(G.path(5), range(5))
-    np.testing.assert_allclose(bc, [0, 6, 8, 6, 0])
+    G.assert_bc_close(bc, [0, 6, 8, 6, 0])
     bc = gk.bc_batch(G.star(6), range(7))
     assert bc[0] == pytest.approx(30.0) and np.all(bc[1:] == 0)
 
@@ -132,16 +132,14 @@ def test_bc_closed_forms_and_host_buffers(gk, cuda):
 def test_bc_directed(gk, orc, cuda):
     A = G.random_csr(300, 300, 0.02, seed=11)
     src = np.arange(0, 300, 7)
-    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), G.brandes_f64(A, src), rtol=BC_RTOL,
-                               atol=1e-9)
+    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), G.brandes_f64(A, src), BC_RTOL)
 
 
 def test_bc_heavy_vertices(gk, orc, cuda):
     # hub of degree > 512 goes to the CTA-per-vertex kernels
     A = G.from_edges(2000, [(0, i) for i in range(1, 2000)] + [(i, i + 1) for i in range(1, 1999, 3)])
     src = np.arange(0, 2000, 17)
-    np.testing.assert_allclose(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), rtol=BC_RTOL,
-                               atol=1e-9)
+    G.assert_bc_close(gk.bc_batch(dev(A), src).cpu().numpy(), orc.bc_f64(A, src), BC_RTOL)
 
 
 @pytest.mark.parametrize("shape", [0, 1, -1])
@@ -157,7 +155,7 @@ def test_bc_forward_shapes_match_oracle(gk, orc, cuda, shape):
         ms, feat, bc = sched.bc_tune(dev(A), src, shape)
         assert len(ms) >= 1 and np.all(ms > 0) and feat.shape == (len(ms), 8)
         want = orc.bc_f64(A, src) if A.m != 300 else G.brandes_f64(A, src)
-        np.testing.assert_allclose(bc.cpu().numpy(), want, rtol=BC_RTOL, atol=1e-9)
+        G.assert_bc_close(bc.cpu().numpy(), want, BC_RTOL)
 
 
 def test_bc_graph_loop_matches_host_loop(gk, cuda):
@@ -173,11 +171,11 @@ def test_bc_graph_loop_matches_host_loop(gk, cuda):
         host = gk.bc_batch(A, src).cpu().numpy()
     finally:
         lib.gk_prof_enable(0)
-    np.testing.assert_allclose(host, ref, rtol=BC_RTOL, atol=1e-9)
+    G.assert_bc_close(host, ref, BC_RTOL)
     if os.path.exists(sched.BC_MODEL_PATH):
         sched.load_bc_model()
         learned = gk.bc_batch(A, src, sched="learned").cpu().numpy()
-        np.testing.assert_allclose(learned, ref, rtol=BC_RTOL, atol=1e-9)
+        G.assert_bc_close(learned, ref, BC_RTOL)
 
 
 def test_bc_golden(gk, cuda):

@@ -68,7 +68,7 @@ def test_allocation_failures_leave_the_library_usable(gk, orc, cuda):
     src = np.arange(24)
     want_bc = orc.bc_f64(A, src)
     drive_failures(gk, lambda: gk.bc_batch(A, src),
-                   lambda got: np.testing.assert_allclose(got, want_bc, rtol=1e-12, atol=1e-9))
+                   lambda got: G.assert_bc_close(got, want_bc))
     graphs = [gk.lower_host(gk.gen_rmat(6 + i % 3, 16, seed=70 + i)) for i in range(6)]
     want = np.array([orc.tc_lower(x) for x in graphs], dtype=np.uint64)
     drive_failures(gk, lambda: gk.tc_count_batched(graphs),
@@ -88,5 +88,5 @@ def test_counts_and_scores_survive_relabelling(gk, orc, cuda, seed):
     src = np.arange(0, A.m, 37)
     bc_a = gk.bc_batch(A, src)
     bc_p = gk.bc_batch(P, perm[src])
-    np.testing.assert_allclose(bc_p[perm], bc_a, rtol=1e-12, atol=1e-9)
+    G.assert_bc_close(bc_p[perm], bc_a)
     assert np.all(bc_a >= 0)

@@ -227,6 +227,52 @@ def test_device_transforms(gk, orc, cuda):
     np.testing.assert_array_equal(Th.col, tcol)
 
 
+def _lower_with_diagonal(n, density, seed):
+    """A square L holding entries at and below the diagonal, random values."""
+    R = G.random_csr(n, n, density, seed, values=True)
+    rp, col, val = np.asarray(R.rowptr), np.asarray(R.col), np.asarray(R.val)
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    keep = col <= rows
+    rows, col, val = rows[keep], col[keep], val[keep]
+    nrp = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=nrp[1:])
+    return G.Csr(n, n, nrp, col.astype(np.int32), val.astype(np.int32), int(len(col)))
+
+
+def test_device_symm_and_adjacency(gk, orc, cuda):
+    """build_symm_from_lower and build_adjacency_matrix on the GPU against the
+    reference's own (include/matrix.h:643-696): patterns bit-exact, the
+    transpose's entry first on equal columns, values carried."""
+    A = gk.gen_rmat(12, 8, seed=5)
+    Lh = gk.lower_host(A)
+    S = gk.build_symm_from_lower(dev(Lh))
+    np.testing.assert_array_equal(S.rowptr.cpu().numpy(), A.rowptr)
+    np.testing.assert_array_equal(S.col.cpu().numpy(), A.col)
+    for L in (Lh, _lower_with_diagonal(300, 0.05, 4)):
+        want_rp, want_col = orc.ref_build_symm(L) if orc.ref_available() else (None, None)
+        for X in (dev(L), L):  # device and host buffers
+            S = gk.build_symm_from_lower(X, with_values=True)
+            rp = S.rowptr.cpu().numpy() if hasattr(S.rowptr, "cpu") else S.rowptr
+            col = S.col.cpu().numpy() if hasattr(S.col, "cpu") else S.col
+            val = S.val.cpu().numpy() if hasattr(S.val, "cpu") else S.val
+            if want_rp is not None:
+                np.testing.assert_array_equal(rp, want_rp)
+                np.testing.assert_array_equal(col, want_col)
+            # values: an entry below the diagonal is L's, above it L^T's; on the
+            # diagonal the transpose's copy comes first, then L's (equal values)
+            dense = G.dense_of(L)
+            rows = np.repeat(np.arange(L.m), np.diff(rp))
+            want_val = np.where(col <= rows, dense[rows, col], dense[col, rows])
+            np.testing.assert_array_equal(val, want_val)
+    Gv = G.random_csr(200, 300, 0.03, 8, values=True)
+    for X in (dev(Gv), Gv):
+        Adj = gk.build_adjacency_matrix(X)
+        np.testing.assert_array_equal(np.asarray(Adj.rowptr.cpu() if hasattr(Adj.rowptr, "cpu") else Adj.rowptr),
+                                      Gv.rowptr)
+        np.testing.assert_array_equal(np.asarray(Adj.col.cpu() if hasattr(Adj.col, "cpu") else Adj.col), Gv.col)
+        assert np.all(np.asarray(Adj.val.cpu() if hasattr(Adj.val, "cpu") else Adj.val) == 1)
+
+
 def test_learned_without_model_is_an_error(gk, cuda):
     if gk.load().gk_sched_has_model():
         pytest.skip("a model is loaded in this process")

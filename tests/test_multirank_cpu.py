@@ -132,3 +132,17 @@ def test_reference_arm_on_a_small_workload(monkeypatch):
     line = json.loads(buf.getvalue())
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "edges/s"
     assert line["cpu_baseline"]["kind"] == "reference" and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["config"] == bench.tc_config(bench.WORKLOADS["tc14"], 16384, line["config"]["nnz_lower"])
+
+
+def test_reference_arm_does_not_load_the_product_library():
+    """The reference arm generates its input with the oracle's restatement of
+    the generator: libgk_b200.so is never mapped into its process."""
+    import subprocess
+    code = ("import runpy, sys, os; os.environ['RANK'] = '0'; os.environ['WORLD_SIZE'] = '1'; "
+            "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'tc14', '--steps', '1', '--warmup', '0']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "print('MAPPED', 'libgk_b200' in open('/proc/self/maps').read())")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "MAPPED False" in out.stdout and '"impl": "reference"' in out.stdout

@@ -335,3 +335,22 @@ def test_dense_operators_vs_reference(orc, seed):
         cols = np.asarray(M.col[M.rowptr[i]:M.rowptr[i + 1]])
         want[i, cols] = D[dense_s[i]].sum(axis=0)[cols]
     np.testing.assert_allclose(orc.mxmm_spd(S, D, M), want, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("scale,seed", [(8, 1), (12, 3), (15, 2)])
+def test_oracle_generator_equals_library_builder(gk, orc, scale, seed):
+    """The oracle's own restatement of the seeded generators (used by the
+    CPU side of the benchmark, which must not load the product library)
+    gives the library builder's graphs bit for bit."""
+    A = gk.gen_rmat(scale, 16, seed=seed)
+    B = orc.gen_rmat(scale, 16, seed)
+    np.testing.assert_array_equal(A.rowptr, B.rowptr)
+    np.testing.assert_array_equal(A.col, B.col)
+    L = gk.lower_host(A)
+    Lo = orc.gen_rmat(scale, 16, seed, lower=True)
+    np.testing.assert_array_equal(L.rowptr, Lo.rowptr)
+    np.testing.assert_array_equal(L.col, Lo.col)
+    E = gk.gen_er(3000 + scale, 20000, seed=seed)
+    Eo = orc.gen_er(3000 + scale, 20000, seed)
+    np.testing.assert_array_equal(E.rowptr, Eo.rowptr)
+    np.testing.assert_array_equal(E.col, Eo.col)

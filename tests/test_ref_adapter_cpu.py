@@ -9,12 +9,12 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INCLUDE = os.environ.get("GK_REFERENCE_INCLUDE", "/root/reference/include")
 
 
-def test_reference_adapter_compiles_and_links(gk, tmp_path):
-    if not os.path.isdir(REF_INCLUDE):
+def test_reference_adapter_compiles_and_links(gk, orc, tmp_path):
+    if not orc.reference_present():
         pytest.skip("reference headers not present on this host")
+    REF_INCLUDE = os.path.join(orc.REFERENCE_DIR, "include")
     cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
     lib = os.path.dirname(gk.LIB_PATH)
     exe = tmp_path / "adapter"

@@ -51,6 +51,25 @@ def test_noalloc_device_output(gk, cuda):
     assert int(out.item()) == gk.tc_count(L)
 
 
+def test_noalloc_empty_graphs(gk, cuda):
+    """An empty graph gives 0; its one-entry row pointer must still be in
+    device memory, since the content check reads it on the device."""
+    import torch
+    from tests import graphs as G
+    for n in (0, 5):
+        E = G.empty(n)
+        status, got = noalloc_count(gk, E.to("cuda"))
+        assert status == 0 and got == 0, gk.load().gk_last_error_string()
+        status, _ = noalloc_count(gk, E)  # host rowptr {0, ...}
+        assert status == 1 and b"device memory" in gk.load().gk_last_error_string()
+    torch.cuda.synchronize()
+    # the library still works after the refusals
+    A = gk.gen_rmat(8, 16, seed=2, device="cuda")
+    L = gk.extract_lower(A)
+    status, got = noalloc_count(gk, L)
+    assert status == 0 and got == gk.tc_count(L)
+
+
 def test_noalloc_refuses_what_it_cannot_hold(gk, cuda):
     A = gk.gen_rmat(21, 4, seed=1, device="cuda")  # 2,097,152 rows > 1,048,576
     L = gk.extract_lower(A)
