@@ -181,6 +181,40 @@ __device__ __forceinline__ T block_sum(T v, T *red) {
 
 __device__ __forceinline__ int ilog2_u64(unsigned long long x) { return x ? 63 - __clzll(x) : 0; }
 
+// ----- asynchronous staging of a sorted mask chunk into shared memory ---------
+// cp.async copies global memory to shared memory without passing through
+// registers; the copies of a chunk are issued by all of the group's lanes and
+// complete at cp_async_wait_all() (a hardware wait, no polling loop).
+__device__ __forceinline__ void cp_async_4(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Element offset (0..3) that puts a shared-memory copy of src on the same
+// position modulo 16 bytes as src, so that its interior can move in 16-byte
+// copies.  The shared buffer must hold n + 3 elements.
+__device__ __forceinline__ int stage_phase(const int32_t *src) {
+    return static_cast<int>((reinterpret_cast<uintptr_t>(src) >> 2) & 3);
+}
+
+// dst[0, n) = src[0, n) by cp.async, issued by `lane` of `lanes` threads; dst
+// is congruent to src modulo 16 bytes (stage_phase).  The 16-byte-aligned
+// interior moves in 16-byte copies, the ragged ends (at most 3 elements each)
+// in 4-byte copies, so no copy reads outside src[0, n).
+__device__ __forceinline__ void stage_ints_async(int *dst, const int32_t *src, int n, int lane, int lanes) {
+    int head = (4 - stage_phase(src)) & 3;
+    if (head > n) head = n;
+    const int body = (n - head) & ~3;
+    for (int q = lane; q < head; q += lanes) cp_async_4(dst + q, src + q);
+    for (int q = head + 4 * lane; q < head + body; q += 4 * lanes) cp_async_16(dst + q, src + q);
+    for (int q = head + body + lane; q < n; q += lanes) cp_async_4(dst + q, src + q);
+}
+
 // Number of A-entry splits of a row in the block kinds.
 __host__ __device__ __forceinline__ int64_t num_splits(int64_t work, int64_t a_len, int split_log2) {
     if (split_log2 <= 0 || a_len <= 1) return 1;

@@ -76,7 +76,9 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
         int c0, c1;  // mask positions covered
         int lo_col, hi_col;
         int *keys = smem;
-        int *acc = smem + ((KIND == K_MSA_BLOCK) ? (ACC ? WIN / 32 : 0) : CAP);
+        // MCA: the sorted keys sit at an offset of 0..3 elements (cp.async
+        // staging keeps them congruent to the source modulo 16 bytes)
+        int *acc = smem + ((KIND == K_MSA_BLOCK) ? (ACC ? WIN / 32 : 0) : (KIND == K_MCA_BLOCK ? CAP + 4 : CAP));
         unsigned *bits = reinterpret_cast<unsigned *>(smem);
         unsigned *filt = reinterpret_cast<unsigned *>(smem + CAP * (ACC ? 2 : 1));
         bool cut;
@@ -113,10 +115,12 @@ __global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THRE
             c0 = static_cast<int>(ch) * CHUNK;
             c1 = min(mlen, c0 + CHUNK);
             if constexpr (KIND == K_MCA_BLOCK) {
-                for (int q = threadIdx.x; q < c1 - c0; q += NT) {
-                    keys[q] = mc[c0 + q];
-                    if (ACC) acc[q] = 0;
-                }
+                // the sorted chunk is copied verbatim: cp.async staging
+                keys = smem + stage_phase(mc + c0);
+                stage_ints_async(keys, mc + c0, c1 - c0, threadIdx.x, NT);
+                if (ACC)
+                    for (int q = threadIdx.x; q < c1 - c0; q += NT) acc[q] = 0;
+                cp_async_wait_all();
             } else {
                 for (int s = threadIdx.x; s < CAP; s += NT) {
                     keys[s] = EMPTY_KEY;

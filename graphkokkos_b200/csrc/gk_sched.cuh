@@ -30,7 +30,7 @@ struct BinStats {
 };
 
 // ---- variants -----------------------------------------------------------------
-enum Kind : int { K_HASH_GROUP = 0, K_HASH_BLOCK = 1, K_MCA_GROUP = 2, K_MCA_BLOCK = 3, K_MSA_BLOCK = 4 };
+enum Kind : int { K_HASH_GROUP = 0, K_HASH_BLOCK = 1, K_MCA_GROUP = 2, K_MCA_BLOCK = 3, K_MSA_BLOCK = 4, K_SEARCH = 5 };
 
 struct Variant {
     int kind;
@@ -47,7 +47,7 @@ struct Variant {
     int lowb;       // block HASH kinds: log2 of the low-column range the filter maps exactly (0: none)
 };
 
-constexpr int NV = 17;
+constexpr int NV = 19;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
 // Tables are bucketed (four slots per 16-byte load).  The small ones run at
 // load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
@@ -55,6 +55,12 @@ constexpr int NV = 17;
 // entry) send only filter candidates to the table; variants 12-14 have none
 // and look every streamed element up in the table directly, which wins on
 // rows where a large share of the elements are mask columns.
+// Variant 17 (K_SEARCH) does not stream B rows: a warp per row looks each mask
+// column inside B_k's column range up in B_k by binary search (mask chunks of
+// 256 columns in shared memory), which wins where mask rows are short and B
+// rows long.  Variant 18 is variant 5 with quarter-warp (8-lane) sub-groups, for
+// B rows shorter than a half-warp's 64-element vector step (small graphs of a
+// many-graph batch).
 // columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum,
 // exact low-column bits (variants 15, 16: the filter maps columns below 2^lowb
 // one to one, so a hit there needs no table lookup when only sums are kept)
@@ -76,6 +82,8 @@ constexpr int NV = 17;
     {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3  , 0},   \
     {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18},  \
     {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 14, 2, 3  , 15},  \
+    {K_SEARCH,      32, 32,   256,   256,   256,   256,   0,  0, 2, 0  , 0},   \
+    {K_HASH_BLOCK, 128,  8,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -110,6 +118,8 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 14: return qm >= 8;
         case 15: return qm >= 8;
         case 16: return true;
+        case 17: return qm <= 8;  // binary-search lookups: mask rows below 512 columns
+        case 18: return qm <= 11;
         default: return false;
     }
 }

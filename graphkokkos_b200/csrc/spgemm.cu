@@ -13,7 +13,7 @@
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
 //                   get their item count (mask chunks x A-entry splits)
 //  5. one persistent kernel per variant over its rows / items (the catalogue
-//     of 17 variants is the table in gk_sched.cuh):
+//     of 19 variants is the table in gk_sched.cuh):
 //       HASH_GROUP  4, 8 or 32 threads per row, the mask row's columns in a
 //                   shared-memory bucketed hash set (slot = accumulator)
 //       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
@@ -25,6 +25,8 @@
 //       MCA_BLOCK   one CTA per item, up to 16K sorted mask columns
 //       MSA_BLOCK   one CTA per item, dense column-window accumulator
 //                   (the reference's MSA, matrix_la.h:611-631) or bitmap
+//       SEARCH      a warp per row, each mask column inside B_k's column range
+//                   looked up in B_k by binary search (gk_ksearch.cuh)
 // B rows are streamed with 16-byte vector loads; mask chunks that do not cover
 // a whole mask row only stream the part of B_k inside the chunk's column range
 // (group-cooperative search).  Integer terms are summed in 32-bit wrapping
@@ -148,7 +150,7 @@ __global__ void k_bin_rows(DevCsr A, DevCsr M, const int64_t *work, const int32_
 __device__ __forceinline__ int64_t items_of_row(int v, bool write, int64_t mlen, int64_t alen, int64_t w,
                                                 const int32_t *mcol_row) {
     const Variant V = c_variants[v];
-    if (V.kind == K_HASH_GROUP || V.kind == K_MCA_GROUP) return 1;
+    if (V.kind == K_HASH_GROUP || V.kind == K_MCA_GROUP || V.kind == K_SEARCH) return 1;
     int64_t nch;
     if (V.kind == K_MSA_BLOCK) {
         const int lw = write ? V.cap_write : V.cap;
@@ -482,9 +484,13 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
     const int sg = lane / SUB, sl = lane % SUB;
-    int *keys = smem + g * CAP;
-    int *acc = smem + NG * CAP + g * CAP;
-    unsigned *filt = reinterpret_cast<unsigned *>(smem + NG * CAP * (ACC ? 2 : 1)) + g * FW;
+    // MCA: each group's sorted keys get 4 spare slots (cp.async staging puts
+    // them at an offset of 0..3 elements, congruent to the source mod 16 bytes)
+    constexpr int KST = MCA ? CAP + 4 : CAP;
+    int *const keys0 = smem + g * KST;
+    int *keys = keys0;
+    int *acc = smem + NG * KST + g * CAP;
+    unsigned *filt = reinterpret_cast<unsigned *>(smem + NG * KST + NG * CAP * (ACC ? 1 : 0)) + g * FW;
     const unsigned gmask = group_mask<G>();
     const int begin = p.voff[p.v], end = p.voff[p.v + 1];
     unsigned long long local = 0;
@@ -524,10 +530,11 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
             const int c1 = min(mlen, c0 + CHUNK);
             const int clen = c1 - c0;
             if (MCA) {
-                for (int q = lane; q < clen; q += G) {
-                    keys[q] = mc[c0 + q];
-                    if (ACC) acc[q] = 0;
-                }
+                keys = keys0 + stage_phase(mc + c0);
+                stage_ints_async(keys, mc + c0, clen, lane, G);
+                if (ACC)
+                    for (int q = lane; q < clen; q += G) acc[q] = 0;
+                cp_async_wait_all();
             } else {
                 for (int q = c0 + lane; q < c1; q += G) {
                     const int x = mc[q];
@@ -599,6 +606,7 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_group(KArgs p) {
 }
 
 #include "gk_kblock.cuh"
+#include "gk_ksearch.cuh"
 
 // ---------------------------------------------------------------------------
 // host side: launching one variant
@@ -611,7 +619,10 @@ constexpr size_t smem_bytes(bool write) {
         const int ng = nt / X.G;
         const int cap = (X.kind == K_MCA_GROUP) ? X.chunk : X.cap;
         const size_t filter = (X.kind == K_HASH_GROUP && X.flog > 0) ? (size_t(1) << X.flog) / 8 : 0;
-        return size_t(ng) * (size_t(cap) * 4 * (write ? 2 : 1) + filter);
+        const size_t stage_pad = (X.kind == K_MCA_GROUP) ? 16 : 0;  // cp.async alignment slots
+        return size_t(ng) * (size_t(cap) * 4 * (write ? 2 : 1) + filter + stage_pad);
+    } else if constexpr (X.kind == K_SEARCH) {
+        return size_t(NT_GROUP / 32) * size_t(write ? X.cap_write : X.cap) * 4 * (write ? 2 : 1);
     } else if constexpr (X.kind == K_MSA_BLOCK) {
         if (write) return (size_t(1) << X.cap_write) / 8 + (size_t(1) << X.cap_write) * 4;
         return (size_t(1) << X.cap) / 8;
@@ -619,7 +630,8 @@ constexpr size_t smem_bytes(bool write) {
         const int cap = write ? X.cap_write : X.cap;
         const size_t filter =
             (X.kind == K_HASH_BLOCK && X.flog > 0) ? ((size_t(1) << X.lowb) + (size_t(1) << X.flog)) / 8 : 0;
-        return size_t(cap) * 4 * (write ? 2 : 1) + filter;
+        const size_t stage_pad = (X.kind == K_MCA_BLOCK) ? 16 : 0;  // cp.async alignment slots
+        return size_t(cap) * 4 * (write ? 2 : 1) + filter + stage_pad;
     }
 }
 
@@ -638,6 +650,9 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         constexpr int CAPV = MCA ? X.chunk : X.cap;
         fn = k_group<X.G, X.sub, NTV, CAPV, X.chunk, MCA, (MCA ? 0 : X.flog), EPI, VAL>;
         nt = NTV;
+    } else if constexpr (X.kind == K_SEARCH) {
+        fn = k_search<NT_GROUP, (W ? X.cap_write : X.cap), EPI, VAL>;
+        nt = NT_GROUP;
     } else {
         constexpr int CAPV = W ? X.cap_write : X.cap;
         constexpr int CHV = W ? X.chunk_write : X.chunk;
@@ -691,6 +706,8 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 14: return launch_variant_v<14>(a, epi, val, sms, s, launch);
         case 15: return launch_variant_v<15>(a, epi, val, sms, s, launch);
         case 16: return launch_variant_v<16>(a, epi, val, sms, s, launch);
+        case 17: return launch_variant_v<17>(a, epi, val, sms, s, launch);
+        case 18: return launch_variant_v<18>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -717,7 +734,8 @@ size_t spgemm_scratch_bytes(int64_t m) {
 static const char *const kVariantRange[NV] = {
     "gk:variant 0",  "gk:variant 1",  "gk:variant 2",  "gk:variant 3",  "gk:variant 4",  "gk:variant 5",
     "gk:variant 6",  "gk:variant 7",  "gk:variant 8",  "gk:variant 9",  "gk:variant 10", "gk:variant 11",
-    "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16"};
+    "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16", "gk:variant 17",
+    "gk:variant 18"};
 
 // ---------------------------------------------------------------------------
 // driver

@@ -87,6 +87,22 @@ def read_model_bin(path):
     return np.frombuffer(raw[12:12 + 4 * n], dtype="<f4").astype(np.float32)
 
 
+def widen_outputs(w, nv_old, nv_new, bias, nf=8, h=32):
+    """A model of nv_old outputs as one of nv_new: the new outputs get zero
+    weights and the given bias (a large bias: a variant predicted never to
+    win, so that the widened model keeps the old choices until it is
+    retrained with timings of the new variants)."""
+    w = np.asarray(w, dtype=np.float32)
+    o = h * nf + h + h * h + h
+    W3 = w[o:o + nv_old * h].reshape(nv_old, h)
+    b3 = w[o + nv_old * h:o + nv_old * h + nv_old]
+    tail = w[o + nv_old * h + nv_old:]
+    assert tail.shape[0] == 2 * nf
+    W3n = np.concatenate([W3, np.zeros((nv_new - nv_old, h), dtype=np.float32)])
+    b3n = np.concatenate([b3, np.full(nv_new - nv_old, bias, dtype=np.float32)])
+    return np.concatenate([w[:o], W3n.ravel(), b3n, tail]).astype(np.float32)
+
+
 def load_model(path=MODEL_PATH):
     """Loads the learned row-bin model through the library's file loader (the
     call a C or C++ host makes); `path` may name the .npz or the .bin."""
@@ -481,6 +497,37 @@ def build_graph(spec):
     return api.gen_er(spec["n"], spec["nedges"], seed=spec["seed"], device="cuda")
 
 
+def add_variants(recs, variants, reps=2, log=print):
+    """Times `variants` on the bins of the saved sweep records (where the bin
+    admits them), re-building each record's graph, and merges the timings in
+    place: a variant added to the catalogue joins the training data without
+    re-measuring the others."""
+    import torch
+    from . import api
+    specs = dict(TRAIN_GRAPHS)
+    specs.update({name + "-ktruss": spec for name, spec in KTRUSS_GRAPHS})
+    for name in dict.fromkeys(r["graph"] for r in recs):
+        mine = [r for r in recs if r["graph"] == name]
+        spec = specs[name]
+        G = build_graph(spec)
+        mode = mine[0]["mode"]
+        if mode == 0:
+            L = api.extract_lower(G)
+            del G
+            G = L
+        t0 = time.time()
+        for r in mine:
+            for v in variants:
+                if allowed(r["bin"], v):
+                    r["ms"][v] = time_bin(G, mode, r["bin"], v, reps)
+            best = min(r["ms"], key=r["ms"].get)
+            log(f"  {name} bin {r['bin']:3d} " + " ".join(f"v{v} {r['ms'].get(v, float('nan')):8.3f}" for v in variants)
+                + f"  plain v{r['plain']} {r['ms'].get(r['plain'], float('nan')):8.3f}  best v{best} {r['ms'][best]:8.3f}")
+        log(f"  {name}: {len(mine)} bins in {time.time() - t0:.1f} s")
+        del G
+        torch.cuda.empty_cache()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", action="store_true", help="sweep the training graphs, train and save the model")
@@ -490,6 +537,9 @@ def main():
     ap.add_argument("--max-scale", type=int, default=24)
     ap.add_argument("--out", default=MODEL_DIR, help="directory for model.npz (and sweep.npz with --train)")
     ap.add_argument("--data", default=DATA_PATH, help="sweep to train from with --retrain")
+    ap.add_argument("--add-variants", default="",
+                    help="comma-separated variant ids: time them on every bin of the saved sweep (re-building "
+                         "its graphs), merge the timings into the sweep, then train")
     ap.add_argument("--train-bc", action="store_true", help="sweep the BC graphs, train and save the BC model")
     ap.add_argument("--retrain-bc", action="store_true", help="train the BC model from the saved BC sweep")
     args = ap.parse_args()
@@ -516,6 +566,11 @@ def main():
             recs += sweep(A, 1, name + "-ktruss")
             del A
             torch.cuda.empty_cache()
+        save_dataset(recs, data_path)
+    if args.add_variants:
+        data_path = os.path.join(args.out, "sweep.npz")
+        recs = load_dataset(args.data)
+        add_variants(recs, [int(v) for v in args.add_variants.split(",")])
         save_dataset(recs, data_path)
     recs = load_dataset(data_path)
     X, Y, M = to_dataset(recs)
