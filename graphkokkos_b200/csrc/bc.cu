@@ -56,9 +56,12 @@ namespace gk {
 #ifndef GK_BC_TMAX
 #define GK_BC_TMAX 16
 #endif
-// Resident CTAs per SM the light level kernels are register-capped for.
+// Resident CTAs per SM the light level kernels are register-capped for: 4 CTAs
+// of 8 warps (32 warps per SM, 64 registers a thread), which their gathers of
+// scattered FP64 words need for latency hiding; their accumulators live in
+// shared memory (SmemAcc, 32 KB a CTA).
 #ifndef GK_BC_MINB
-#define GK_BC_MINB 2
+#define GK_BC_MINB 4
 #endif
 constexpr int BC_HEAVY = 512;
 constexpr int BC_NW_HEAVY = 8;  // T=16: 8*16*32 doubles = 32 KB of static shared memory
@@ -133,6 +136,14 @@ __device__ __forceinline__ void load_words_rw(const uint32_t *p, uint32_t (&w)[T
 #pragma unroll
     for (int t = 0; t < T; ++t) w[t] = p[t];
 }
+
+// The light level kernels keep each lane's FP64 accumulators of the T source
+// words in shared memory (the warp's slice, word t of lane l at 32 t + l:
+// conflict-free) instead of 2T registers, which would cap their residency.
+struct SmemAcc {
+    double *p;
+    __device__ __forceinline__ double &operator[](int t) const { return p[32 * t]; }
+};
 
 // One atomic per block and counter.
 __device__ __forceinline__ void add_level_stats(unsigned long long n, unsigned long long e, unsigned long long b,
@@ -255,10 +266,10 @@ __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_
 // ---------------------------------------------------------------------------
 // Lanes test 32 neighbours' frontier words at a time; each neighbour carrying
 // a needed bit then has its sigma words added by the lanes of those sources.
-template <int T>
+template <int T, class AccT>
 __device__ __forceinline__ bool pull_sigma(const DevCsr &AT, int64_t ebeg, int64_t e1, int64_t estep,
                                            const uint32_t *__restrict__ Fd, const uint32_t (&need)[T],
-                                           const double *__restrict__ sigma, int W, int lane, double (&acc)[T]) {
+                                           const double *__restrict__ sigma, int W, int lane, AccT &acc) {
     bool any = false;
     for (int64_t base = ebeg; base < e1; base += estep) {
         const int64_t e = base + lane;
@@ -293,18 +304,21 @@ __device__ __forceinline__ bool pull_sigma(const DevCsr &AT, int64_t ebeg, int64
 
 // New level bits, sigma and visited words of vertex i; returns the number of
 // new (vertex, source) pairs (valid in every lane).
-template <int T>
-__device__ __forceinline__ int pull_emit(int64_t i, int W, int lane, const uint32_t (&vis)[T],
-                                         const double (&acc)[T], uint32_t *Fn, uint32_t *V, double *sigma) {
+// V[i] is written only by the warp that emits vertex i, so its visited words
+// are re-read here rather than carried in registers through the gather.
+template <int T, class AccT>
+__device__ __forceinline__ int pull_emit(int64_t i, int W, int lane, const AccT &acc, uint32_t *Fn, uint32_t *V,
+                                         double *sigma) {
     int c = 0;
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        const uint32_t nb = __ballot_sync(0xFFFFFFFFu, acc[t] != 0.0);
+        const double a = acc[t];
+        const uint32_t nb = __ballot_sync(0xFFFFFFFFu, a != 0.0);
         c += __popc(nb);
-        if ((nb >> lane) & 1u) sigma[i * W + 32 * t + lane] = acc[t];
+        if ((nb >> lane) & 1u) sigma[i * W + 32 * t + lane] = a;
         if (lane == t) {
             Fn[i * T + t] = nb;
-            V[i * T + t] = vis[t] | nb;
+            V[i * T + t] |= nb;
         }
     }
     return c;
@@ -318,25 +332,26 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_pull(DevCsr AT, DevCsr A
     const uint32_t *__restrict__ Fd = st->fptr[d];
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
+    __shared__ double s_acc[8][T][32];
+    SmemAcc acc{&s_acc[threadIdx.x >> 5][0][lane]};
     unsigned long long n = 0, e = 0, b = 0;
     for (int64_t base = grab_vertices(&st->cur_pull, lane); base < AT.m; base = grab_vertices(&st->cur_pull, lane))
     for (int64_t i = base, iend = min(base + BC_GRAB, AT.m); i < iend; ++i) {
         const int64_t e0 = AT.rp[i], e1 = AT.rp[i + 1];
         if (e0 == e1 || e1 - e0 > BC_HEAVY) continue;
-        uint32_t vis[T], need[T];
-        load_words<T>(V + i * T, vis);
+        uint32_t need[T];
+        load_words<T>(V + i * T, need);
         uint32_t open = 0;
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-            need[t] = ~vis[t] & act[t];
+            need[t] = ~need[t] & act[t];
             open |= need[t];
         }
         if (!open) continue;
-        double acc[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
         if (!pull_sigma<T>(AT, e0, e1, 32, Fd, need, sigma, W, lane, acc)) continue;
-        const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
+        const int c = pull_emit<T>(i, W, lane, acc, Fn, V, sigma);
         if (c && lane == 0) {
             ++n;
             e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
@@ -421,7 +436,7 @@ __global__ void __launch_bounds__(256) k_bc_pull_heavy_emit(DevCsr A, HeavySet h
 #pragma unroll
             for (int t = 0; t < T; ++t) acc[t] += partials[(int64_t)it * W + 32 * t + lane];
         }
-        const int c = pull_emit<T>(i, W, lane, vis, acc, Fn, V, sigma);
+        const int c = pull_emit<T>(i, W, lane, acc, Fn, V, sigma);
         if (c && lane == 0) {
             ++n;
             e += static_cast<unsigned long long>(A.rp[i + 1] - A.rp[i]);
@@ -588,10 +603,10 @@ __global__ void k_bc_rinit(int64_t m, const BcState *st, const double *sigma, do
     }
 }
 
-template <int T>
+template <int T, class AccT>
 __device__ __forceinline__ void pull_r(const DevCsr &A, int64_t ebeg, int64_t e1, int64_t estep,
                                        const uint32_t *__restrict__ Fn, const uint32_t (&fv)[T],
-                                       const double *__restrict__ R, int W, int lane, double (&sum)[T]) {
+                                       const double *__restrict__ R, int W, int lane, AccT &sum) {
     for (int64_t base = ebeg; base < e1; base += estep) {
         const int64_t e = base + lane;
         int w = 0;
@@ -621,8 +636,8 @@ __device__ __forceinline__ void pull_r(const DevCsr &A, int64_t ebeg, int64_t e1
     }
 }
 
-template <int T>
-__device__ __forceinline__ void bwd_emit(int64_t v, int W, int lane, const uint32_t (&fv)[T], const double (&sum)[T],
+template <int T, class AccT>
+__device__ __forceinline__ void bwd_emit(int64_t v, int W, int lane, const uint32_t (&fv)[T], const AccT &sum,
                                          const double *sigma, double *R, double *bc) {
     double tot = 0.0;
 #pragma unroll
@@ -647,6 +662,8 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
     const uint32_t *__restrict__ Fd = st->fptr[d];
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
+    __shared__ double s_sum[8][T][32];
+    SmemAcc sum{&s_sum[threadIdx.x >> 5][0][lane]};
     for (int64_t base = grab_vertices(&st->cur_bwd, lane); base < A.m; base = grab_vertices(&st->cur_bwd, lane))
     for (int64_t v = base, vend = min(base + BC_GRAB, A.m); v < vend; ++v) {
         const int64_t e0 = A.rp[v], e1 = A.rp[v + 1];
@@ -657,7 +674,6 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
 #pragma unroll
         for (int t = 0; t < T; ++t) any |= fv[t];
         if (!any) continue;
-        double sum[T];
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
         pull_r<T>(A, e0, e1, 32, Fn, fv, R, W, lane, sum);
