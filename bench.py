@@ -230,34 +230,66 @@ def golden_large(kind, **match):
     return None
 
 
-def tc_sampler(L_host, kind, target_s):
-    """Stride of a row sample of L whose reference TC takes about target_s
-    seconds on this host's cores.  A first sample of about 64 rows runs twice
-    (the first also faults in the per-thread scratch pool, as Kokkos' pool
-    would be warm in a long run); its second time and entry count give the
-    per-entry rate the stride is sized from.  Returns (stride, probe)."""
+_ROW_ORDER = {}
+
+
+def sample_rows(L_host, nrows, seed):
+    """A sample of nrows rows of L for CPU timing, representative of the
+    graph's work: the rows sorted by their work (the B entries their A
+    entries stream, sum over k in L_i of nnz(L_k)) are taken systematically,
+    every (m / nrows)-th from a seeded random start, so every work quantile is
+    represented in proportion.  The work of an RMAT row is heavy-tailed, and
+    its ID carries its degree in its bits (multiples of large powers of two
+    are hubs), so strided or small uniform samples give rates that differ by
+    tens of percent from sample to sample.  Returned sorted."""
+    key = id(L_host)
+    if key not in _ROW_ORDER:
+        rp = np.asarray(L_host.rowptr, dtype=np.int64)
+        col = np.asarray(L_host.col)[: int(rp[-1])]
+        deg = np.diff(rp)
+        cs = np.zeros(len(col) + 1, dtype=np.int64)
+        np.cumsum(deg[col], out=cs[1:])
+        work = cs[rp[1:]] - cs[rp[:-1]]
+        _ROW_ORDER[key] = np.argsort(work, kind="stable")
+    order = _ROW_ORDER[key]
+    m = len(order)
+    nrows = min(m, max(1, nrows))
+    step = m / nrows
+    start = np.random.default_rng(seed).random() * step
+    pos = np.minimum(m - 1, (start + step * np.arange(nrows)).astype(np.int64))
+    return np.sort(order[pos])
+
+
+def tc_sampler(L_host, kind, target_s, seed=0):
+    """Number of sampled rows of L (sample_rows) whose reference TC takes about
+    target_s seconds on this host's cores.  A first sample of 2,048 rows runs
+    twice (the first also faults in the per-thread scratch pool, as Kokkos'
+    pool would be warm in a long run); its second time gives the per-row cost
+    the sample is sized from.  Returns (rows, probe)."""
     import oracle
-    stride = max(1, L_host.m // 64)
-    oracle.tc_row_stride(L_host, stride, 0, kind=kind)
-    cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
-    probe = {"rows": (L_host.m + stride - 1) // stride, "entries": nz, "seconds": sec}
-    if sec > 0 and nz > 0:
-        stride = max(1, min(stride, int(stride * sec / target_s)))
-    return stride, probe
+    rows0 = sample_rows(L_host, 2048, seed + 1000)
+    oracle.tc_rows_sample(L_host, rows0, kind=kind)
+    cnt, nz, sec, thr = oracle.tc_rows_sample(L_host, rows0, kind=kind)
+    probe = {"rows": len(rows0), "entries": nz, "seconds": sec}
+    nrows = len(rows0)
+    if sec > 0:
+        nrows = int(len(rows0) * target_s / sec)
+    return max(1, min(L_host.m, nrows)), probe
 
 
 def cpu_baseline(L_host, target_s=12.0):
     """The reference's mxmm_msa (oracle/_ref, via the Kokkos-API shim) on a
-    strided row sample of L, on this host's cores; falls back to the port.
-    The sample is compacted to its rows, so the reference's per-call costs
-    that scale with the row count follow the sample (oracle/ref_oracle.cpp,
-    ref_tc_row_stride)."""
+    work-representative row sample of L (sample_rows), on this host's cores;
+    falls back to the port.  The sample is compacted to its rows, so the reference's per-call
+    costs that scale with the row count follow the sample
+    (oracle/ref_oracle.cpp, ref_tc_rows_sample)."""
     import oracle
     kind = "reference" if oracle.ref_available() else "port"
-    stride, probe = tc_sampler(L_host, kind, target_s)
-    cnt, nz, sec, thr = oracle.tc_row_stride(L_host, stride, 0, kind=kind)
+    nrows, probe = tc_sampler(L_host, kind, target_s)
+    cnt, nz, sec, thr = oracle.tc_rows_sample(L_host, sample_rows(L_host, nrows, 1), kind=kind)
     return {"value": nz / sec if sec > 0 else None, "unit": "edges/s", "cores": thr, "kind": kind,
-            "sample": f"rows i % {stride} == 0 of L ({nz} of {L_host.nnz} entries), {sec:.1f} s, "
+            "sample": f"{nrows} rows of L taken systematically in order of their work (seed 1; {nz} of "
+                      f"{L_host.nnz} entries), {sec:.1f} s, "
                       f"C<S> = S·L then sum (reference bracket src/main.cpp:74-85); a {probe['rows']}-row "
                       f"sample ({probe['entries']} entries) took {probe['seconds']:.3f} s"}
 
@@ -652,7 +684,7 @@ def run_tcbatch(args, wl, torch, gk, dist, rank, world):
             done_nz, sec, thr = 0, 0.0, 1
             for g in sample:
                 Lh = Hs[g].numpy()
-                cnt, nz, s_, thr = oracle.tc_row_stride(Lh, 1, 0, kind=kind)
+                cnt, nz, s_, thr = oracle.tc_all_rows(Lh, kind=kind)
                 assert cnt == int(ref[g]), f"graph {g}: CPU count {cnt} != GPU {int(ref[g])}"
                 done_nz += nz
                 sec += s_
@@ -743,7 +775,7 @@ def reference_tcbatch(args, wl, world):
         for g in range(i, len(specs), 97):
             kind_g, a, b, seed = specs[g]
             Lg = oracle.gen_rmat(a, b, seed, lower=True) if kind_g == "rmat" else oracle.gen_er(a, b, seed, lower=True)
-            _, nz, sec, thr = oracle.tc_row_stride(Lg, 1, 0, kind=kind)
+            _, nz, sec, thr = oracle.tc_all_rows(Lg, kind=kind)
             nz_tot += nz
             sec_tot += sec
             if sec_tot > max(2.0, 120.0 / max(1, args.steps + args.warmup)):
@@ -779,11 +811,11 @@ def main_reference(args):
     kind = "reference" if oracle.ref_available() else "port"
     # size the per-step sample so that warmup + steps stay within a few minutes
     per_step_budget = max(2.0, 150.0 / max(1, args.steps + args.warmup))
-    stride, probe = tc_sampler(L, kind, per_step_budget)
+    nrows, probe = tc_sampler(L, kind, per_step_budget)
     vals = []
     thr = 1
     for i in range(args.warmup + args.steps):
-        cnt, nz, sec, thr = oracle.tc_row_stride(L, stride, i % stride, kind=kind)
+        cnt, nz, sec, thr = oracle.tc_rows_sample(L, sample_rows(L, nrows, 100 + i), kind=kind)
         if i >= args.warmup:
             vals.append(nz / sec)
     v = statistics.median(vals)
@@ -793,8 +825,9 @@ def main_reference(args):
             "generator, bit-identical to the library's)", "impl": "reference",
             "config": tc_config(wl, L.m, L.nnz), "sched": "n/a",
             "cpu_baseline": {"value": v, "unit": "edges/s", "cores": thr, "kind": kind,
-                             "sample": f"each step: rows i % {stride} == offset of L (compacted), reference "
-                                       f"mxmm_msa + sum; a {probe['rows']}-row sample took "
+                             "sample": f"each step: {nrows} rows of L taken systematically in order of their "
+                                       f"work (seed 100 + step, compacted), reference mxmm_msa + sum; a "
+                                       f"{probe['rows']}-row sample took "
                                        f"{probe['seconds']:.3f} s"},
             "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

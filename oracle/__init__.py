@@ -97,21 +97,28 @@ def tc_rows(L, row_begin, row_end):
     return int(out.value)
 
 
-def tc_row_stride(L, stride, offset=0, kind="reference"):
-    """Bounded CPU sample of triangle counting: rows i % stride == offset.
+def tc_rows_sample(L, rows, kind="reference"):
+    """Bounded CPU sample of triangle counting over the listed rows of L (for
+    a representative sample: a sorted uniform random choice of rows).
     kind "reference": the reference's mxmm_msa (oracle/_ref); "port": the
     restatement.  Returns (partial count, sampled nnz, seconds, threads)."""
     m, _, rp, col, _ = _host(L)
+    rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int64))
     out = ctypes.c_int64(0) if kind == "reference" else ctypes.c_uint64(0)
     nz = ctypes.c_int64(0)
     sec = ctypes.c_double(0.0)
     lib = ref() if kind == "reference" else port()
-    fn = lib.ref_tc_row_stride if kind == "reference" else lib.orc_tc_row_stride
-    r = fn(I64(m), _p(rp), _p(col), I64(stride), I64(offset), ctypes.byref(out), ctypes.byref(nz), ctypes.byref(sec))
+    fn = lib.ref_tc_rows_sample if kind == "reference" else lib.orc_tc_rows_sample
+    r = fn(I64(m), _p(rp), _p(col), I64(len(rows)), _p(rows), ctypes.byref(out), ctypes.byref(nz), ctypes.byref(sec))
     if r != 0:
-        raise RuntimeError("tc_row_stride failed")
+        raise RuntimeError("tc_rows_sample failed")
     threads = ref().ref_get_threads() if kind == "reference" else os.cpu_count()
     return int(out.value), int(nz.value), float(sec.value), int(threads)
+
+
+def tc_all_rows(L, kind="reference"):
+    """tc_rows_sample over every row of L."""
+    return tc_rows_sample(L, np.arange(L.m, dtype=np.int64), kind)
 
 
 def tc_merge(L):

@@ -205,9 +205,10 @@ int orc_tc_rows(int64_t m, const int64_t *rp, const int32_t *col, int64_t row_be
     return 0;
 }
 
-// Bounded sample: rows i with i % stride == offset (B = all of L).
-int orc_tc_row_stride(int64_t m, const int64_t *rp, const int32_t *col, int64_t stride, int64_t offset,
-                      uint64_t *out, int64_t *sample_nnz, double *seconds) {
+// Bounded sample: the listed rows (B = all of L), e.g. a uniform random
+// sample of the rows.
+int orc_tc_rows_sample(int64_t m, const int64_t *rp, const int32_t *col, int64_t nrows, const int64_t *rows,
+                       uint64_t *out, int64_t *sample_nnz, double *seconds) {
     const double t0 = omp_get_wtime();
     uint64_t total = 0;
     int64_t nz = 0;
@@ -215,7 +216,8 @@ int orc_tc_row_stride(int64_t m, const int64_t *rp, const int32_t *col, int64_t 
     {
         std::vector<uint8_t> mark(static_cast<size_t>(m), 0);
 #pragma omp for schedule(dynamic, 16)
-        for (int64_t i = offset; i < m; i += stride) {
+        for (int64_t r = 0; r < nrows; ++r) {
+            const int64_t i = rows[r];
             nz += rp[i + 1] - rp[i];
             for (int64_t j = rp[i]; j < rp[i + 1]; ++j) mark[col[j]] = 1;
             uint64_t c = 0;

@@ -381,41 +381,39 @@ int ref_tc_rows(int parallel, int64_t m, const int64_t *rp, const int32_t *col,
 }
 
 // Bounded sample for CPU timing: C<S> = S·L through the reference mxmm_msa,
-// with S = the rows i of L with i % stride == offset, compacted to a matrix of
-// those rows only (r rows, m columns): the reference's per-call costs that
-// scale with the row count (the copy of M's pattern into C, matrix_la.h:564-568,
-// and the serial work split, :590-596) then follow the sample, not the whole
-// graph, so the measured rate is the rate of the reference's row loop.  The
-// shim's per-thread scratch is kept between calls and not zero-filled here, as
-// Kokkos' own scratch pool is (the MSA clears its accumulator at the mask
-// columns before each row, :614-616).  Returns the sum of C (the sampled rows'
-// share of the triangle count) and the number of sampled L entries; `seconds`
-// receives the time inside mxmm_msa plus the sum, the reference's own bracket
-// (src/main.cpp:74-85).
-int ref_tc_row_stride(int64_t m, const int64_t *rp, const int32_t *col, int64_t stride, int64_t offset,
-                      int64_t *out, int64_t *sample_nnz, double *seconds) {
+// with S = the listed rows of L (a uniform random sample of the rows, sorted),
+// compacted to a matrix of those rows only (nrows rows, m columns): the
+// reference's per-call costs that scale with the row count (the copy of M's
+// pattern into C, matrix_la.h:564-568, and the serial work split, :590-596)
+// then follow the sample, not the whole graph, so the measured rate is the
+// rate of the reference's row loop.  The shim's per-thread scratch is kept
+// between calls and not zero-filled here, as Kokkos' own scratch pool is (the
+// MSA clears its accumulator at the mask columns before each row, :614-616).
+// Returns the sum of C (the sampled rows' share of the triangle count) and the
+// number of sampled L entries; `seconds` receives the time inside mxmm_msa
+// plus the sum, the reference's own bracket (src/main.cpp:74-85).
+int ref_tc_rows_sample(int64_t m, const int64_t *rp, const int32_t *col, int64_t nrows, const int64_t *rows,
+                       int64_t *out, int64_t *sample_nnz, double *seconds) {
     try {
         spMtx<int> L = make_mtx(m, m, rp, col, nullptr);
-        int64_t nz = 0, r = 0;
-        for (int64_t i = offset; i < m; i += stride) {
-            nz += rp[i + 1] - rp[i];
-            ++r;
-        }
+        int64_t nz = 0;
+        for (int64_t r = 0; r < nrows; ++r) nz += rp[rows[r] + 1] - rp[rows[r]];
         if (nz == 0) {  // no entries: the sample's count is 0 (see msa_guarded)
             *out = 0;
             *sample_nnz = 0;
             *seconds = 0.0;
             return 0;
         }
-        spMtx<int> S(static_cast<size_t>(r), static_cast<size_t>(m), static_cast<size_t>(nz));
-        int64_t pos = 0, row = 0;
+        spMtx<int> S(static_cast<size_t>(nrows), static_cast<size_t>(m), static_cast<size_t>(nz));
+        int64_t pos = 0;
         S.Rst(0) = 0;
-        for (int64_t i = offset; i < m; i += stride) {
+        for (int64_t r = 0; r < nrows; ++r) {
+            const int64_t i = rows[r];
             for (int64_t j = rp[i]; j < rp[i + 1]; ++j) {
                 S.Col(pos) = col[j];
                 S.Val(pos++) = 1;
             }
-            S.Rst(++row) = static_cast<int>(pos);
+            S.Rst(r + 1) = static_cast<int>(pos);
         }
         spMtx<int> C;
         ThreadCap cap(nz);
