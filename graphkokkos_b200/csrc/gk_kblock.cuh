@@ -13,8 +13,20 @@
 //    entry's B-row bounds are loaded while the current B row streams.
 #pragma once
 
+// Resident CTAs a block kind is register-capped for: GK_LB_THREADS / NT, or
+// fewer when its shared memory (table, accumulators, filter) admits fewer per
+// SM anyway, so that the large-table kinds get the registers of the residency
+// they can actually reach.
+__host__ __device__ constexpr int block_min_ctas(int nt, int kind, int cap, int flog, int lowb, bool acc) {
+    const int by_threads = GK_LB_THREADS / nt < 1 ? 1 : GK_LB_THREADS / nt;
+    if (kind != K_HASH_BLOCK) return by_threads;
+    const long smem = long(cap) * 4 * (acc ? 2 : 1) + (flog > 0 ? ((1l << lowb) + (1l << flog)) / 8 : 0);
+    const int by_smem = int((228l * 1024) / (smem + 1024));
+    return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
+}
+
 template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL, int LOWB = 0>
-__global__ void __launch_bounds__(NT, (GK_LB_THREADS / NT) < 1 ? 1 : (GK_LB_THREADS / NT)) k_block(KArgs p) {
+__global__ void __launch_bounds__(NT, block_min_ctas(NT, KIND, CAP, FLOG, LOWB, EPI == EPI_WRITE)) k_block(KArgs p) {
     constexpr bool ACC = (EPI == EPI_WRITE);
     constexpr int NW = NT / 32;
     constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;  // MSA: CAP = log2 window width

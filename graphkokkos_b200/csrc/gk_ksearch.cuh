@@ -18,23 +18,14 @@
 //    lanes: each lane computes its entry's pair count, a warp scan gives the
 //    offsets, and every lane takes pairs lane, lane+32, ... locating the pair's
 //    A entry by a five-step search over the scan held in the lanes' registers
-//    (shuffles).  No lane idles on an A entry with few pairs.
+//    (shuffles).  No lane idles on an A entry with few pairs.  A lane runs two
+//    pairs' binary searches interleaved (two dependent-load chains in flight:
+//    the kernel is bound by the latency of those loads).
 //  * Mask rows longer than CAP are taken in chunks of CAP columns; a pair is
 //    seen in exactly one chunk, so chunking adds no lookups.
 //  * Integer terms are summed exactly as in the other kinds (32-bit wrapping
 //    per lane, 64-bit row totals).
 #pragma once
-
-// Last position in [lo, lo + len) whose value is <= x, for sorted a with
-// a[lo] <= x (len >= 1): ceil(log2 len) dependent loads.
-__device__ __forceinline__ int64_t last_le(const int32_t *__restrict__ a, int64_t lo, int64_t len, int x) {
-    while (len > 1) {
-        const int64_t half = len >> 1;
-        lo = (__ldg(a + lo + half) <= x) ? lo + half : lo;
-        len -= half;
-    }
-    return lo;
-}
 
 // First index q in [0, n) of the sorted shared-memory array k with k[q] >= x
 // (strict = false) or k[q] > x (strict = true); n when there is none.
@@ -59,6 +50,14 @@ __device__ __forceinline__ int64_t shfl64(int64_t v, int src) {
     const int hi = __shfl_sync(0xFFFFFFFFu, static_cast<int>(v >> 32), src);
     return (static_cast<int64_t>(hi) << 32) | static_cast<uint32_t>(lo);
 }
+
+// One (A entry, mask column) lookup of the search kernel.
+struct Pair {
+    int64_t lo, len;  // remaining search range in B.col
+    int c, q;         // the mask column and its position in the chunk
+    uint32_t av;      // the A entry's value (1 for patterns)
+    bool live;
+};
 
 template <int NT, int CAP, int EPI, bool VAL>
 __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
@@ -125,28 +124,54 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
                 }
                 const int total = __shfl_sync(FULL, incl, 31);
                 const int excl = incl - n;
-                for (int pb = 0; pb < total; pb += 32) {
-                    const int pp = pb + lane;
-                    // the pair's A entry: the first lane j whose inclusive
-                    // count exceeds pp (binary lifting over the lanes)
-                    int j = 0;
+                // two pairs per lane per round (pairs pb + lane and
+                // pb + 32 + lane), their binary searches interleaved so that
+                // two dependent-load chains are in flight per lane
+                for (int pb = 0; pb < total; pb += 64) {
+                    Pair P[2];
 #pragma unroll
-                    for (int s = 16; s > 0; s >>= 1) {
-                        const int v = __shfl_sync(FULL, incl, j + s - 1);
-                        if (v <= pp) j += s;
+                    for (int h = 0; h < 2; ++h) {
+                        const int pp = pb + 32 * h + lane;
+                        // the pair's A entry: the first lane j whose inclusive
+                        // count exceeds pp (binary lifting over the lanes)
+                        int j = 0;
+#pragma unroll
+                        for (int s = 16; s > 0; s >>= 1) {
+                            const int v = __shfl_sync(FULL, incl, j + s - 1);
+                            if (v <= pp) j += s;
+                        }
+                        const int ex_j = __shfl_sync(FULL, excl, j);
+                        const int qlo_j = __shfl_sync(FULL, qlo, j);
+                        const int64_t b0_j = shfl64(b0, j), b1_j = shfl64(b1, j);
+                        P[h].av = VAL ? static_cast<uint32_t>(__shfl_sync(FULL, static_cast<int>(av), j)) : 1u;
+                        P[h].live = pp < total;
+                        P[h].q = P[h].live ? qlo_j + (pp - ex_j) : 0;
+                        P[h].c = P[h].live ? mk[P[h].q] : 0;
+                        P[h].lo = b0_j;
+                        P[h].len = P[h].live ? b1_j - b0_j : 1;
                     }
-                    const int ex_j = __shfl_sync(FULL, excl, j);
-                    const int qlo_j = __shfl_sync(FULL, qlo, j);
-                    const int64_t b0_j = shfl64(b0, j), b1_j = shfl64(b1, j);
-                    const uint32_t av_j = VAL ? static_cast<uint32_t>(__shfl_sync(FULL, static_cast<int>(av), j)) : 1u;
-                    if (pp < total) {
-                        const int q = qlo_j + (pp - ex_j);
-                        const int c = mk[q];
-                        const int64_t pos = last_le(p.B.col, b0_j, b1_j - b0_j, c);
-                        if (__ldg(p.B.col + pos) == c) {
-                            const uint32_t w =
-                                (VAL && p.B.val) ? av_j * static_cast<uint32_t>(__ldg(p.B.val + pos)) : av_j;
-                            if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + q), w);
+                    // last position with B.col <= c in each pair's B row
+                    // (B.col[lo] <= c holds: c lies inside the row's range)
+                    while (P[0].len > 1 || P[1].len > 1) {
+                        int x[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                            if (P[h].len > 1) x[h] = __ldg(p.B.col + P[h].lo + (P[h].len >> 1));
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                            if (P[h].len > 1) {
+                                const int64_t half = P[h].len >> 1;
+                                if (x[h] <= P[h].c) P[h].lo += half;
+                                P[h].len -= half;
+                            }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        if (P[h].live && __ldg(p.B.col + P[h].lo) == P[h].c) {
+                            const uint32_t w = (VAL && p.B.val)
+                                                   ? P[h].av * static_cast<uint32_t>(__ldg(p.B.val + P[h].lo))
+                                                   : P[h].av;
+                            if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + P[h].q), w);
                             else cnt += w;
                         }
                     }

@@ -47,7 +47,7 @@ struct Variant {
     int lowb;       // block HASH kinds: log2 of the low-column range the filter maps exactly (0: none)
 };
 
-constexpr int NV = 19;
+constexpr int NV = 20;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
 // Tables are bucketed (four slots per 16-byte load).  The small ones run at
 // load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
@@ -60,7 +60,10 @@ constexpr int NV = 19;
 // 256 columns in shared memory), which wins where mask rows are short and B
 // rows long.  Variant 18 is variant 5 with quarter-warp (8-lane) sub-groups, for
 // B rows shorter than a half-warp's 64-element vector step (small graphs of a
-// many-graph batch).
+// many-graph batch).  Variant 19 is variant 8 (mask chunks of 8,192 columns
+// for hub rows) with variant 15's exact map of the columns below 2^18: a hub
+// row's mask and the B rows it streams concentrate on low vertex IDs, where a
+// hit then costs one bit test instead of a divergent table lookup.
 // columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum,
 // exact low-column bits (variants 15, 16: the filter maps columns below 2^lowb
 // one to one, so a hit there needs no table lookup when only sums are kept)
@@ -84,6 +87,7 @@ constexpr int NV = 19;
     {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 14, 2, 3  , 15},  \
     {K_SEARCH,      32, 32,   256,   256,   256,   256,   0,  0, 2, 0  , 0},   \
     {K_HASH_BLOCK, 128,  8,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 16, 1, 3  , 18},  \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -120,6 +124,7 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 16: return true;
         case 17: return qm <= 8;  // binary-search lookups: mask rows below 512 columns
         case 18: return qm <= 11;
+        case 19: return qm >= 10;
         default: return false;
     }
 }

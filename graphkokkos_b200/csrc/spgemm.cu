@@ -13,7 +13,7 @@
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
 //                   get their item count (mask chunks x A-entry splits)
 //  5. one persistent kernel per variant over its rows / items (the catalogue
-//     of 19 variants is the table in gk_sched.cuh):
+//     of 20 variants is the table in gk_sched.cuh):
 //       HASH_GROUP  4, 8 or 32 threads per row, the mask row's columns in a
 //                   shared-memory bucketed hash set (slot = accumulator)
 //       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
@@ -708,6 +708,7 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 16: return launch_variant_v<16>(a, epi, val, sms, s, launch);
         case 17: return launch_variant_v<17>(a, epi, val, sms, s, launch);
         case 18: return launch_variant_v<18>(a, epi, val, sms, s, launch);
+        case 19: return launch_variant_v<19>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -735,7 +736,7 @@ static const char *const kVariantRange[NV] = {
     "gk:variant 0",  "gk:variant 1",  "gk:variant 2",  "gk:variant 3",  "gk:variant 4",  "gk:variant 5",
     "gk:variant 6",  "gk:variant 7",  "gk:variant 8",  "gk:variant 9",  "gk:variant 10", "gk:variant 11",
     "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16", "gk:variant 17",
-    "gk:variant 18"};
+    "gk:variant 18", "gk:variant 19"};
 
 // ---------------------------------------------------------------------------
 // driver
