@@ -195,17 +195,21 @@ def tc_roofline(gk, torch, L, sched, peak, peak_kind, call=None, traffic_key=Non
     traffic = traffic_for(dom, d["work"]) if traffic_key == "tc24" else None
     return {"kernel": f"masked SpGEMM variant {dom}", "bound": "hbm", "achieved": round(achieved, 1),
             "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic, "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
-            "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "rows": x["rows"]}
+            "traffic": traffic, "traffic_source": "RMAT-22 capture scaled by streamed entries" if traffic else None,
+            "launch_ms": round(d["ms"], 3), "bytes_per_launch": d["bytes"],
+            "variants": {str(v): {"ms": round(x["ms"], 3), "work": x["work"], "rows": x["rows"],
+                                  "frac": round(x["bytes"] / (x["ms"] / 1e3) / 1e9 / peak, 4) if x["ms"] > 0 else None}
                          for v, x in sorted(per.items())}}
 
 
 def traffic_for(variant, work):
-    """DRAM bytes (read + write) of one launch of `variant` streaming `work`
-    B entries: the full-size ncu capture of that kernel on the same graph
-    (profiles/tc_rmat24_traffic.json), scaled by the streamed entries when the
-    schedule has since moved rows onto or off the variant."""
-    path = os.path.join(ROOT, "profiles", "tc_rmat24_traffic.json")
+    """Estimated DRAM bytes (read + write) of one launch of `variant`
+    streaming `work` B entries on triangle counting RMAT-24: the variant's
+    DRAM bytes per streamed entry in a one-pass ncu capture of the same
+    schedule on RMAT-22 (profiles/tc_rmat22_dram.json), times the entries of
+    this launch.  The capture's graph is 16x smaller, so more of its B rows
+    stay in L2: the estimate is a lower bound."""
+    path = os.path.join(ROOT, "profiles", "tc_rmat22_dram.json")
     try:
         with open(path) as f:
             rec = json.load(f).get(str(variant))
@@ -213,7 +217,7 @@ def traffic_for(variant, work):
         return None
     if not rec or not rec.get("work"):
         return None
-    return int(round(rec["traffic"] * work / rec["work"]))
+    return int(round((rec["dram_read"] + rec["dram_write"]) * work / rec["work"]))
 
 
 GOLDEN_LARGE = os.path.join(ROOT, "tests", "golden", "large.json")
@@ -345,6 +349,14 @@ def run_tc(args, wl, torch, gk, dist, rank, world):
     if rank == 0:
         peak, peak_kind = hbm_peak()
         line["roofline"] = tc_roofline(gk, torch, L, head, peak, peak_kind, traffic_key=args.workload)
+        # the whole call against the same roofline: the reference formulation's
+        # algorithmic bytes of every row (4 W + 20 nnz(L) + 16 (m + 1) + 8)
+        # over the device time of one step
+        work_all = sum(v["work"] for v in line["roofline"]["variants"].values())
+        step_bytes = 4 * work_all + 20 * L.nnz + 16 * (L.m + 1) + 8
+        step_gbs = step_bytes / (res[head]["ms_per_step"] / 1e3) / 1e9
+        line["roofline"]["step"] = {"bytes": step_bytes, "achieved": round(step_gbs, 1),
+                                    "frac": round(step_gbs / peak, 4)}
         # end to end through the public API with host buffers: the H2D copy of
         # L (pinned) and the D2H read of the count are inside the timed region
         Lh = L.to("cpu")

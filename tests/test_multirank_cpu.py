@@ -87,10 +87,11 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
 def test_roofline_traffic_scales_with_streamed_entries():
     sys.path.insert(0, ROOT)
     import bench
-    rec = json.load(open(os.path.join(ROOT, "profiles", "tc_rmat24_traffic.json")))["6"]
-    assert bench.traffic_for(6, rec["work"]) == rec["traffic"]  # the captured launch itself
-    assert bench.traffic_for(6, rec["work"] // 2) == pytest.approx(rec["traffic"] / 2, rel=1e-9)
-    assert bench.traffic_for(3, 10) is None  # no capture of that kernel
+    rec = json.load(open(os.path.join(ROOT, "profiles", "tc_rmat22_dram.json")))["6"]
+    captured = rec["dram_read"] + rec["dram_write"]
+    assert bench.traffic_for(6, rec["work"]) == captured  # the captured launch itself
+    assert bench.traffic_for(6, rec["work"] * 16) == pytest.approx(captured * 16, rel=1e-9)
+    assert bench.traffic_for(3, 10) is None  # no capture of that kernel (it ran no rows)
 
 
 def test_clock_sampler_parses_nvidia_smi_lines(tmp_path, monkeypatch):
