@@ -17,16 +17,20 @@
 // fewer when its shared memory (table, accumulators, filter) admits fewer per
 // SM anyway, so that the large-table kinds get the registers of the residency
 // they can actually reach.
-__host__ __device__ constexpr int block_min_ctas(int nt, int kind, int cap, int flog, int lowb, bool acc) {
+__host__ __device__ constexpr int block_min_ctas(int nt, int kind, int cap, int flog, int lowb, bool acc,
+                                                 int comp = 0) {
     const int by_threads = GK_LB_THREADS / nt < 1 ? 1 : GK_LB_THREADS / nt;
     if (kind != K_HASH_BLOCK) return by_threads;
-    const long smem = long(cap) * 4 * (acc ? 2 : 1) + (flog > 0 ? ((1l << lowb) + (1l << flog)) / 8 : 0);
+    const long smem = long(cap) * 4 * (acc ? 2 : 1) + (flog > 0 ? ((1l << lowb) + (1l << flog)) / 8 : 0) +
+                      (comp ? long(nt) * 8 * 4 : 0);
     const int by_smem = int((228l * 1024) / (smem + 1024));
     return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
 }
 
-template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL, int LOWB = 0>
-__global__ void __launch_bounds__(NT, block_min_ctas(NT, KIND, CAP, FLOG, LOWB, EPI == EPI_WRITE)) k_block(KArgs p) {
+template <int NT, int KIND, int SUB, int CAP, int CHUNK, int SPLIT, int FLOG, int NB, int EPI, bool VAL, int LOWB = 0,
+          int COMP = 0>
+__global__ void __launch_bounds__(NT, block_min_ctas(NT, KIND, CAP, FLOG, LOWB, EPI == EPI_WRITE, COMP))
+    k_block(KArgs p) {
     constexpr bool ACC = (EPI == EPI_WRITE);
     constexpr int NW = NT / 32;
     constexpr int WIN = (KIND == K_MSA_BLOCK) ? (1 << CAP) : 0;  // MSA: CAP = log2 window width
@@ -166,6 +170,8 @@ __global__ void __launch_bounds__(NT, block_min_ctas(NT, KIND, CAP, FLOG, LOWB, 
             const int probe_arg = (KIND == K_MSA_BLOCK) ? lo_col : clen;
             const int *pkeys = (KIND == K_MSA_BLOCK) ? reinterpret_cast<const int *>(bits) : keys;
             const unsigned *pfilt = FWORDS > 0 ? filt : nullptr;
+            // candidate queue of this sub-group (COMP kinds): 8 elements per lane
+            int *queue = COMP ? reinterpret_cast<int *>(filt + FWORDS) + (threadIdx.x / SUB) * 8 * SUB : nullptr;
             auto fetch = [&]() -> int64_t {
                 int tt = 0;
                 if (sl == 0) tt = atomicAdd(&s_next, 1);
@@ -192,8 +198,9 @@ __global__ void __launch_bounds__(NT, block_min_ctas(NT, KIND, CAP, FLOG, LOWB, 
                             }
                         }
                         if (!skip)
-                            stream_row<SUB, CAP, PKV, ACC, VAL, (FWORDS > 0 ? FLOG : 0), (FWORDS > 0 ? LOWB : 0)>(
-                                p, cur.b0, cur.b1, sl, cur.av, pkeys, acc, probe_arg, cnt, pfilt, hi_col);
+                            stream_row<SUB, CAP, PKV, ACC, VAL, (FWORDS > 0 ? FLOG : 0), (FWORDS > 0 ? LOWB : 0),
+                                       (FWORDS > 0 ? COMP : 0)>(p, cur.b0, cur.b1, sl, cur.av, pkeys, acc, probe_arg,
+                                                                 cnt, pfilt, hi_col, queue);
                     }
                     tc = tn;
                     tn = tnn;

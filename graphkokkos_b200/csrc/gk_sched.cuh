@@ -45,9 +45,10 @@ struct Variant {
     int batch;      // items a CTA (group kinds: a warp) takes per fetch
     int accum;      // gk_accum family this variant belongs to
     int lowb;       // block HASH kinds: log2 of the low-column range the filter maps exactly (0: none)
+    int comp;       // block HASH kinds: filter candidates packed into a per-warp queue and checked one per lane
 };
 
-constexpr int NV = 20;
+constexpr int NV = 22;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
 // Tables are bucketed (four slots per 16-byte load).  The small ones run at
 // load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
@@ -63,31 +64,36 @@ constexpr int NV = 20;
 // many-graph batch).  Variant 19 is variant 8 (mask chunks of 8,192 columns
 // for hub rows) with variant 15's exact map of the columns below 2^18: a hub
 // row's mask and the B rows it streams concentrate on low vertex IDs, where a
-// hit then costs one bit test instead of a divergent table lookup.
-// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum,
+// hit then costs one bit test instead of a divergent table lookup.  Variants 20
+// and 21 are variants 8 and 15 with the filter candidates of a warp packed into
+// a shared-memory queue and checked one per lane (comp = 1), for rows whose
+// mask covers a large share of the streamed elements.
+// columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum, comp,
 // exact low-column bits (variants 15, 16: the filter maps columns below 2^lowb
 // one to one, so a hit there needs no table lookup when only sums are kept)
 #define GK_VARIANT_TABLE { \
-    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3  , 0},   \
-    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3  , 0},   \
-    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 13, 1, 3  , 0},   \
-    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3  , 0},   \
-    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
-    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
-    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 16, 2, 3  , 0},   \
-    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19, 17, 1, 3  , 0},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3  , 0},   \
-    {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2  , 0},   \
-    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2  , 0},   \
-    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1  , 0},   \
-    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3  , 0},   \
-    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18,  0, 2, 3  , 0},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3  , 0},   \
-    {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18},  \
-    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 14, 2, 3  , 15},  \
-    {K_SEARCH,      32, 32,   256,   256,   256,   256,   0,  0, 2, 0  , 0},   \
-    {K_HASH_BLOCK, 128,  8,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0},   \
-    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 16, 1, 3  , 18},  \
+    {K_HASH_GROUP,   4,  4,    64,    64,    16,    16,   0,  0, 1, 3  , 0, 0},   \
+    {K_HASH_GROUP,   8,  8,   128,   128,    32,    32,   0,  0, 1, 3  , 0, 0},   \
+    {K_HASH_GROUP,  32, 32,   512,   512,   128,   128,   0, 13, 1, 3  , 0, 0},   \
+    {K_HASH_BLOCK,  64, 32,   512,   512,   128,   128,  16, 13, 8, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 128, 32,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 128, 16,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 16, 2, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19, 17, 1, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3  , 0, 0},   \
+    {K_MCA_GROUP,   32, 32,   256,   256,   256,   256,   0,  0, 1, 2  , 0, 0},   \
+    {K_MCA_BLOCK,  512, 32, 16384, 16384, 16384, 16384,  20,  0, 1, 2  , 0, 0},   \
+    {K_MSA_BLOCK,  512, 32,    20,    15,     0,     0,  20,  0, 1, 1  , 0, 0},   \
+    {K_HASH_BLOCK, 256, 32,  8192,  8192,  4096,  4096,  19,  0, 1, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18,  0, 2, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20,  0, 1, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18, 0},  \
+    {K_HASH_BLOCK, 128, 32,  2048,  2048,  1024,  1024,  18, 14, 2, 3  , 15, 0},  \
+    {K_SEARCH,      32, 32,   256,   256,   256,   256,   0,  0, 2, 0  , 0, 0},   \
+    {K_HASH_BLOCK, 128,  8,  1024,  1024,   256,   256,  17, 14, 4, 3  , 0, 0},   \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 16, 1, 3  , 18, 0},  \
+    {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3  , 0, 1},  \
+    {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18, 1}, \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -125,6 +131,8 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 17: return qm <= 8;  // binary-search lookups: mask rows below 512 columns
         case 18: return qm <= 11;
         case 19: return qm >= 10;
+        case 20:
+        case 21: return qm >= 8;
         default: return false;
     }
 }

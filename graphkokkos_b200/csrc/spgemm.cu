@@ -13,7 +13,7 @@
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
 //                   get their item count (mask chunks x A-entry splits)
 //  5. one persistent kernel per variant over its rows / items (the catalogue
-//     of 20 variants is the table in gk_sched.cuh):
+//     of 22 variants is the table in gk_sched.cuh):
 //       HASH_GROUP  4, 8 or 32 threads per row, the mask row's columns in a
 //                   shared-memory bucketed hash set (slot = accumulator)
 //       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
@@ -285,11 +285,14 @@ __device__ __forceinline__ void probe_elem(int x, uint32_t w, const int *keys, i
     }
 }
 
-// Filter bit of x (0/1) and the exact test of a filter candidate.
-template <int FLOG, int LOWB = 0>
-__device__ __forceinline__ uint32_t cand_bit(int x, const unsigned *filt) {
+// Filter bit of x placed at bit E of the result (0 elsewhere): the word's
+// bit h moves to position E by one rotate (funnel shift, amount taken mod 32),
+// and the caller's OR with the other elements' bits folds into the AND.
+template <int FLOG, int LOWB, int E>
+__device__ __forceinline__ uint32_t cand_at(int x, const unsigned *filt) {
     const uint32_t h = filter_pos<FLOG, LOWB>(x);
-    return (filt[h >> 5] >> (h & 31)) & 1u;
+    const uint32_t w = filt[h >> 5];
+    return __funnelshift_r(w, w, h - E) & (1u << E);
 }
 
 template <int CAP, bool ACC>
@@ -302,6 +305,13 @@ __device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, i
     }
 }
 
+// Element e (0..7) of the eight held in x (0..3) and y (4..7).
+__device__ __forceinline__ int elem8(const int4 &x, const int4 &y, int e) {
+    const int lo = (e & 1) ? ((e & 4) ? y.y : x.y) : ((e & 4) ? y.x : x.x);
+    const int hi = (e & 1) ? ((e & 4) ? y.w : x.w) : ((e & 4) ? y.z : x.z);
+    return (e & 2) ? hi : lo;
+}
+
 // Exact lookups of the filter candidates among the eight elements of x, y
 // (bit e of m set = element e passed the filter).  Each lane walks only its
 // own set bits, so a warp iterates as often as its busiest lane has
@@ -309,19 +319,82 @@ __device__ __forceinline__ void exact_hash(int x, uint32_t w, const int *keys, i
 template <int CAP, bool ACC, int LOWB = 0>
 __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int4 &y, uint32_t av,
                                             const int *keys, int *acc, unsigned &cnt) {
+    if constexpr (!ACC && LOWB > 0) {
+        // candidates below 2^LOWB passed an exact bit: counted at once,
+        // without a trip through the per-candidate loop
+        constexpr uint32_t L = 1u << LOWB;
+        const uint32_t low = uint32_t(uint32_t(x.x) < L) | (uint32_t(uint32_t(x.y) < L) << 1) |
+                             (uint32_t(uint32_t(x.z) < L) << 2) | (uint32_t(uint32_t(x.w) < L) << 3) |
+                             (uint32_t(uint32_t(y.x) < L) << 4) | (uint32_t(uint32_t(y.y) < L) << 5) |
+                             (uint32_t(uint32_t(y.z) < L) << 6) | (uint32_t(uint32_t(y.w) < L) << 7);
+        cnt += av * static_cast<uint32_t>(__popc(m & low));
+        m &= ~low;
+    }
     while (m) {
         const int e = __ffs(m) - 1;
         m &= m - 1;
-        const int lo = (e & 1) ? ((e & 4) ? y.y : x.y) : ((e & 4) ? y.x : x.x);
-        const int hi = (e & 1) ? ((e & 4) ? y.w : x.w) : ((e & 4) ? y.z : x.z);
-        const int v = (e & 2) ? hi : lo;
-        if constexpr (!ACC && LOWB > 0) {
-            if (static_cast<uint32_t>(v) < (1u << LOWB)) {  // exact part of the filter: a hit
-                cnt += av;
-                continue;
+        exact_hash<CAP, ACC>(elem8(x, y, e), av, keys, acc, cnt);
+    }
+}
+
+// Vector part of a B row for the high-hit-rate kinds (hub rows, whose mask
+// covers a large share of the B rows they stream): instead of every lane
+// walking its own filter candidates through the table (a loop as long as the
+// busiest lane's candidates), the candidates of the whole sub-group are
+// packed into a shared-memory queue (a scan of the per-lane counts) and
+// checked one per lane.  The loop runs a uniform number of rounds over the
+// row's 16-byte vectors so that the sub-group's collectives stay converged;
+// lanes past the item's last mask column contribute nothing.
+template <int SUB, int CAP, bool ACC, int FLOG, int LOWB>
+__device__ __forceinline__ void stream_vectors_compact(const int4 *__restrict__ base, int n4, int sl, unsigned smask,
+                                                       uint32_t av, const int *keys, int *acc, unsigned &cnt,
+                                                       const unsigned *filt, int hi_col, int *queue) {
+    const int rounds = (n4 + 2 * SUB - 1) / (2 * SUB);
+    bool past = false;
+    for (int it = 0; it < rounds; ++it) {
+        const int q = it * 2 * SUB + sl;
+        int4 x = make_int4(0, 0, 0, 0), y = make_int4(0, 0, 0, 0);
+        uint32_t m = 0;
+        if (!past && q < n4) {
+            x = __ldg(base + q);
+            m = cand_at<FLOG, LOWB, 0>(x.x, filt) | cand_at<FLOG, LOWB, 1>(x.y, filt) |
+                cand_at<FLOG, LOWB, 2>(x.z, filt) | cand_at<FLOG, LOWB, 3>(x.w, filt);
+            if (q + SUB < n4) {
+                y = __ldg(base + q + SUB);
+                m |= cand_at<FLOG, LOWB, 4>(y.x, filt) | cand_at<FLOG, LOWB, 5>(y.y, filt) |
+                     cand_at<FLOG, LOWB, 6>(y.z, filt) | cand_at<FLOG, LOWB, 7>(y.w, filt);
+                past = y.w > hi_col;
+            } else {
+                past = x.w > hi_col;
             }
         }
-        exact_hash<CAP, ACC>(v, av, keys, acc, cnt);
+        if constexpr (!ACC && LOWB > 0) {  // exact part of the filter: hits counted at once
+            constexpr uint32_t L = 1u << LOWB;
+            const uint32_t low = uint32_t(uint32_t(x.x) < L) | (uint32_t(uint32_t(x.y) < L) << 1) |
+                                 (uint32_t(uint32_t(x.z) < L) << 2) | (uint32_t(uint32_t(x.w) < L) << 3) |
+                                 (uint32_t(uint32_t(y.x) < L) << 4) | (uint32_t(uint32_t(y.y) < L) << 5) |
+                                 (uint32_t(uint32_t(y.z) < L) << 6) | (uint32_t(uint32_t(y.w) < L) << 7);
+            cnt += av * static_cast<uint32_t>(__popc(m & low));
+            m &= ~low;
+        }
+        const int nc = __popc(m);
+        int incl = nc;
+#pragma unroll
+        for (int o = 1; o < SUB; o <<= 1) {
+            const int t = __shfl_up_sync(smask, incl, o, SUB);
+            if (sl >= o) incl += t;
+        }
+        const int total = __shfl_sync(smask, incl, SUB - 1, SUB);
+        int w = incl - nc;
+        while (m) {
+            const int e = __ffs(m) - 1;
+            m &= m - 1;
+            queue[w++] = elem8(x, y, e);
+        }
+        __syncwarp(smask);
+        for (int c = sl; c < total; c += SUB) exact_hash<CAP, ACC>(queue[c], av, keys, acc, cnt);
+        __syncwarp(smask);
+        if (__all_sync(smask, past || q >= n4)) break;
     }
 }
 
@@ -331,10 +404,10 @@ __device__ __forceinline__ void exact_cands(uint32_t m, const int4 &x, const int
 // filter without branches and only the candidates take the exact lookup.  A
 // lane stops once its elements pass hi_col, the last mask column of the
 // item (B rows are sorted); elements beyond it could never match.
-template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0, int LOWB = 0>
+template <int SUB, int CAP, int PK, bool ACC, bool VAL, int FLOG = 0, int LOWB = 0, int COMP = 0>
 __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b1, int sl, uint32_t av,
                                            const int *keys, int *acc, int clen, unsigned &cnt,
-                                           const unsigned *filt, int hi_col) {
+                                           const unsigned *filt, int hi_col, int *queue = nullptr) {
     const int32_t *__restrict__ bc = p.B.col;
     if constexpr (PK == PK_HASH && FLOG > 0 && !VAL) {
         if (p.vec) {
@@ -343,15 +416,24 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             if (b0 + sl < h1) probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + b0 + sl), av, keys, acc, clen, cnt, filt);
             const int4 *__restrict__ base = reinterpret_cast<const int4 *>(bc) + (h1 >> 2);
             const int n4 = static_cast<int>((b1 >> 2) - (h1 >> 2));
+            if constexpr (COMP) {
+                stream_vectors_compact<SUB, CAP, ACC, FLOG, LOWB>(base, n4, sl, group_mask<SUB>(), av, keys, acc,
+                                                                   cnt, filt, hi_col, queue);
+                int64_t tl = (b1 >> 2) << 2;
+                if (tl < h1) tl = h1;
+                if (tl + sl < b1)
+                    probe_elem<CAP, PK, ACC, FLOG, LOWB>(__ldg(bc + tl + sl), av, keys, acc, clen, cnt, filt);
+                return;
+            }
             int q = sl;
             bool past = false;  // this lane's elements went beyond the mask's last column
             for (; q + SUB < n4; q += 2 * SUB) {
                 const int4 x = __ldg(base + q);
                 const int4 y = __ldg(base + q + SUB);
-                const uint32_t m = cand_bit<FLOG, LOWB>(x.x, filt) | (cand_bit<FLOG, LOWB>(x.y, filt) << 1) |
-                                   (cand_bit<FLOG, LOWB>(x.z, filt) << 2) | (cand_bit<FLOG, LOWB>(x.w, filt) << 3) |
-                                   (cand_bit<FLOG, LOWB>(y.x, filt) << 4) | (cand_bit<FLOG, LOWB>(y.y, filt) << 5) |
-                                   (cand_bit<FLOG, LOWB>(y.z, filt) << 6) | (cand_bit<FLOG, LOWB>(y.w, filt) << 7);
+                const uint32_t m = cand_at<FLOG, LOWB, 0>(x.x, filt) | cand_at<FLOG, LOWB, 1>(x.y, filt) |
+                                   cand_at<FLOG, LOWB, 2>(x.z, filt) | cand_at<FLOG, LOWB, 3>(x.w, filt) |
+                                   cand_at<FLOG, LOWB, 4>(y.x, filt) | cand_at<FLOG, LOWB, 5>(y.y, filt) |
+                                   cand_at<FLOG, LOWB, 6>(y.z, filt) | cand_at<FLOG, LOWB, 7>(y.w, filt);
                 exact_cands<CAP, ACC, LOWB>(m, x, y, av, keys, acc, cnt);
                 if (y.w > hi_col) {  // B rows are sorted: the rest cannot be mask columns
                     past = true;
@@ -360,8 +442,8 @@ __device__ __forceinline__ void stream_row(const KArgs &p, int64_t b0, int64_t b
             }
             if (!past && q < n4) {
                 const int4 x = __ldg(base + q);
-                const uint32_t m = cand_bit<FLOG, LOWB>(x.x, filt) | (cand_bit<FLOG, LOWB>(x.y, filt) << 1) |
-                                   (cand_bit<FLOG, LOWB>(x.z, filt) << 2) | (cand_bit<FLOG, LOWB>(x.w, filt) << 3);
+                const uint32_t m = cand_at<FLOG, LOWB, 0>(x.x, filt) | cand_at<FLOG, LOWB, 1>(x.y, filt) |
+                                   cand_at<FLOG, LOWB, 2>(x.z, filt) | cand_at<FLOG, LOWB, 3>(x.w, filt);
                 exact_cands<CAP, ACC, LOWB>(m, x, x, av, keys, acc, cnt);
             }
             int64_t tl = (b1 >> 2) << 2;
@@ -631,7 +713,8 @@ constexpr size_t smem_bytes(bool write) {
         const size_t filter =
             (X.kind == K_HASH_BLOCK && X.flog > 0) ? ((size_t(1) << X.lowb) + (size_t(1) << X.flog)) / 8 : 0;
         const size_t stage_pad = (X.kind == K_MCA_BLOCK) ? 16 : 0;  // cp.async alignment slots
-        return size_t(cap) * 4 * (write ? 2 : 1) + filter + stage_pad;
+        const size_t queue = (X.kind == K_HASH_BLOCK && X.comp) ? size_t(X.G) * 8 * 4 : 0;  // candidate queues
+        return size_t(cap) * 4 * (write ? 2 : 1) + filter + stage_pad + queue;
     }
 }
 
@@ -657,7 +740,8 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         constexpr int CAPV = W ? X.cap_write : X.cap;
         constexpr int CHV = W ? X.chunk_write : X.chunk;
         constexpr int FLOGV = (X.kind == K_HASH_BLOCK) ? X.flog : 0;
-        fn = k_block<X.G, X.kind, X.sub, CAPV, CHV, X.split_log2, FLOGV, X.batch, EPI, VAL, (FLOGV > 0 ? X.lowb : 0)>;
+        fn = k_block<X.G, X.kind, X.sub, CAPV, CHV, X.split_log2, FLOGV, X.batch, EPI, VAL, (FLOGV > 0 ? X.lowb : 0),
+                     (FLOGV > 0 ? X.comp : 0)>;
         nt = X.G;
     }
     // resident CTAs per SM, computed once per kernel instance (and device)
@@ -709,6 +793,8 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 17: return launch_variant_v<17>(a, epi, val, sms, s, launch);
         case 18: return launch_variant_v<18>(a, epi, val, sms, s, launch);
         case 19: return launch_variant_v<19>(a, epi, val, sms, s, launch);
+        case 20: return launch_variant_v<20>(a, epi, val, sms, s, launch);
+        case 21: return launch_variant_v<21>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -736,7 +822,7 @@ static const char *const kVariantRange[NV] = {
     "gk:variant 0",  "gk:variant 1",  "gk:variant 2",  "gk:variant 3",  "gk:variant 4",  "gk:variant 5",
     "gk:variant 6",  "gk:variant 7",  "gk:variant 8",  "gk:variant 9",  "gk:variant 10", "gk:variant 11",
     "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16", "gk:variant 17",
-    "gk:variant 18", "gk:variant 19"};
+    "gk:variant 18", "gk:variant 19", "gk:variant 20", "gk:variant 21"};
 
 // ---------------------------------------------------------------------------
 // driver

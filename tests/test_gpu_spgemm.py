@@ -15,7 +15,7 @@ from tests import graphs as G
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-NV = 20
+NV = 22
 
 
 def dev(csr):
