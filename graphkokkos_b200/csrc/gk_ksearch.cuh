@@ -25,6 +25,9 @@
 //    seen in exactly one chunk, so chunking adds no lookups.
 //  * Integer terms are summed exactly as in the other kinds (32-bit wrapping
 //    per lane, 64-bit row totals).
+//  * G lanes per row: a warp (variant 17), or half- and quarter-warps that
+//    take two and four short rows at a time (variants 22 and 23, the small
+//    rows of a many-graph batch), every collective confined to the group.
 #pragma once
 
 // First index q in [0, n) of the sorted shared-memory array k with k[q] >= x
@@ -45,29 +48,36 @@ __device__ __forceinline__ int smem_bound(const int *k, int n, int x) {
     return lo;
 }
 
-__device__ __forceinline__ int64_t shfl64(int64_t v, int src) {
-    const int lo = __shfl_sync(0xFFFFFFFFu, static_cast<int>(v & 0xFFFFFFFF), src);
-    const int hi = __shfl_sync(0xFFFFFFFFu, static_cast<int>(v >> 32), src);
+template <int G>
+__device__ __forceinline__ int64_t shfl64(int64_t v, int src, unsigned gmask) {
+    const int lo = __shfl_sync(gmask, static_cast<int>(v & 0xFFFFFFFF), src, G);
+    const int hi = __shfl_sync(gmask, static_cast<int>(v >> 32), src, G);
     return (static_cast<int64_t>(hi) << 32) | static_cast<uint32_t>(lo);
 }
 
-// One (A entry, mask column) lookup of the search kernel.
+// One (A entry, mask column) lookup of the search kernel: a 32-bit search
+// range inside one B row (B rows hold fewer than 2^31 entries).
 struct Pair {
-    int64_t lo, len;  // remaining search range in B.col
-    int c, q;         // the mask column and its position in the chunk
-    uint32_t av;      // the A entry's value (1 for patterns)
+    const int32_t *row;  // B.col + b0 of the pair's B row
+    int lo, len;         // remaining search range, relative to row
+    int c, q;            // the mask column and its position in the chunk
+    uint32_t av;         // the A entry's value (1 for patterns)
     bool live;
 };
 
-template <int NT, int CAP, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
+// G lanes per row (G = 32: a warp; 16 and 8: two and four short rows per
+// warp), CAP mask columns per chunk in shared memory.
+// Sub-warp groups hold more per-lane state (group masks, shuffle widths):
+// they are register-capped for five CTAs per SM instead of six.
+template <int NT, int G, int CAP, int EPI, bool VAL>
+__global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_THREADS / NT) k_search(KArgs p) {
     constexpr bool ACC = (EPI == EPI_WRITE);
-    constexpr int NWARP = NT / 32;
-    constexpr unsigned FULL = 0xFFFFFFFFu;
+    constexpr int NG = NT / G;
+    const unsigned gmask = group_mask<G>();
     extern __shared__ int smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int *mk = smem + warp * CAP;
-    int *acc = smem + NWARP * CAP + warp * CAP;  // EPI_WRITE only
+    const int grp = threadIdx.x / G, lane = threadIdx.x % G;
+    int *mk = smem + grp * CAP;
+    int *acc = smem + NG * CAP + grp * CAP;  // EPI_WRITE only
     const int begin = p.voff[p.v], end = p.voff[p.v + 1];
     unsigned long long local = 0;
     int cur_key = -1;
@@ -78,7 +88,7 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
     while (true) {
         if (left == 0) {
             if (lane == 0) got = static_cast<int>(atomicAdd(p.fetch + p.v, static_cast<unsigned>(FB)));
-            got = __shfl_sync(FULL, got, 0);
+            got = __shfl_sync(gmask, got, 0, G);
             left = FB;
         }
         const int idx = begin + got + (FB - left);
@@ -91,24 +101,24 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
         unsigned long long rowsum = 0;
         for (int c0 = 0; c0 < mlen; c0 += CAP) {
             const int clen = min(CAP, mlen - c0);
-            for (int q = lane; q < clen; q += 32) {
+            for (int q = lane; q < clen; q += G) {
                 mk[q] = __ldg(p.M.col + m0 + c0 + q);
                 if (ACC) acc[q] = 0;
             }
-            __syncwarp();
+            __syncwarp(gmask);
             const int lo_col = mk[0], hi_col = mk[clen - 1];
             unsigned cnt = 0;
-            for (int64_t tb = a0; tb < a1; tb += 32) {
+            for (int64_t tb = a0; tb < a1; tb += G) {
                 const int64_t t = tb + lane;
-                int64_t b0 = 0, b1 = 0;
-                int qlo = 0, n = 0;
+                int64_t b0 = 0;
+                int blen = 0, qlo = 0, n = 0;
                 uint32_t av = 1u;
                 if (t < a1) {
                     const int k = __ldg(p.A.col + t);
                     b0 = __ldg(p.B.rp + k);
-                    b1 = __ldg(p.B.rp + k + 1);
-                    if (b1 > b0) {
-                        const int first = __ldg(p.B.col + b0), last = __ldg(p.B.col + b1 - 1);
+                    blen = static_cast<int>(__ldg(p.B.rp + k + 1) - b0);
+                    if (blen > 0) {
+                        const int first = __ldg(p.B.col + b0), last = __ldg(p.B.col + b0 + blen - 1);
                         if (last >= lo_col && first <= hi_col) {
                             qlo = smem_bound<false>(mk, clen, first);
                             n = smem_bound<true>(mk, clen, last) - qlo;
@@ -118,78 +128,81 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
                 }
                 int incl = n;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(FULL, incl, o);
+                for (int o = 1; o < G; o <<= 1) {
+                    const int y = __shfl_up_sync(gmask, incl, o, G);
                     if (lane >= o) incl += y;
                 }
-                const int total = __shfl_sync(FULL, incl, 31);
+                const int total = __shfl_sync(gmask, incl, G - 1, G);
                 const int excl = incl - n;
                 // two pairs per lane per round (pairs pb + lane and
-                // pb + 32 + lane), their binary searches interleaved so that
+                // pb + G + lane), their binary searches interleaved so that
                 // two dependent-load chains are in flight per lane
-                for (int pb = 0; pb < total; pb += 64) {
+                for (int pb = 0; pb < total; pb += 2 * G) {
                     Pair P[2];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const int pp = pb + 32 * h + lane;
+                        const int pp = pb + G * h + lane;
                         // the pair's A entry: the first lane j whose inclusive
                         // count exceeds pp (binary lifting over the lanes)
                         int j = 0;
 #pragma unroll
-                        for (int s = 16; s > 0; s >>= 1) {
-                            const int v = __shfl_sync(FULL, incl, j + s - 1);
+                        for (int s = G / 2; s > 0; s >>= 1) {
+                            const int v = __shfl_sync(gmask, incl, j + s - 1, G);
                             if (v <= pp) j += s;
                         }
-                        const int ex_j = __shfl_sync(FULL, excl, j);
-                        const int qlo_j = __shfl_sync(FULL, qlo, j);
-                        const int64_t b0_j = shfl64(b0, j), b1_j = shfl64(b1, j);
-                        P[h].av = VAL ? static_cast<uint32_t>(__shfl_sync(FULL, static_cast<int>(av), j)) : 1u;
+                        const int ex_j = __shfl_sync(gmask, excl, j, G);
+                        const int qlo_j = __shfl_sync(gmask, qlo, j, G);
+                        const int blen_j = __shfl_sync(gmask, blen, j, G);
+                        const int64_t b0_j = shfl64<G>(b0, j, gmask);
+                        P[h].av = VAL ? static_cast<uint32_t>(__shfl_sync(gmask, static_cast<int>(av), j, G)) : 1u;
                         P[h].live = pp < total;
                         P[h].q = P[h].live ? qlo_j + (pp - ex_j) : 0;
                         P[h].c = P[h].live ? mk[P[h].q] : 0;
-                        P[h].lo = b0_j;
-                        P[h].len = P[h].live ? b1_j - b0_j : 1;
+                        P[h].row = p.B.col + b0_j;
+                        P[h].lo = 0;
+                        P[h].len = P[h].live ? blen_j : 1;
                     }
                     // last position with B.col <= c in each pair's B row
-                    // (B.col[lo] <= c holds: c lies inside the row's range)
+                    // (row[0] <= c holds: c lies inside the row's range)
                     while (P[0].len > 1 || P[1].len > 1) {
                         int x[2];
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
-                            if (P[h].len > 1) x[h] = __ldg(p.B.col + P[h].lo + (P[h].len >> 1));
+                            if (P[h].len > 1) x[h] = __ldg(P[h].row + P[h].lo + (P[h].len >> 1));
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
                             if (P[h].len > 1) {
-                                const int64_t half = P[h].len >> 1;
+                                const int half = P[h].len >> 1;
                                 if (x[h] <= P[h].c) P[h].lo += half;
                                 P[h].len -= half;
                             }
                     }
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        if (P[h].live && __ldg(p.B.col + P[h].lo) == P[h].c) {
-                            const uint32_t w = (VAL && p.B.val)
-                                                   ? P[h].av * static_cast<uint32_t>(__ldg(p.B.val + P[h].lo))
-                                                   : P[h].av;
+                        if (P[h].live && __ldg(P[h].row + P[h].lo) == P[h].c) {
+                            const uint32_t w =
+                                (VAL && p.B.val)
+                                    ? P[h].av * static_cast<uint32_t>(__ldg(p.B.val + (P[h].row - p.B.col) + P[h].lo))
+                                    : P[h].av;
                             if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + P[h].q), w);
                             else cnt += w;
                         }
                     }
                 }
             }
-            __syncwarp();
+            __syncwarp(gmask);
             if (ACC) {
-                for (int q = lane; q < clen; q += 32) p.c_val[m0 + c0 + q] = acc[q];
+                for (int q = lane; q < clen; q += G) p.c_val[m0 + c0 + q] = acc[q];
             } else {
                 rowsum += cnt;
             }
-            __syncwarp();
+            __syncwarp(gmask);
         }
         if (EPI == EPI_SUM) local += rowsum;
         if (EPI == EPI_KEYED) {
             const int key = p.row_key ? p.row_key[row] : row;
             if (key != cur_key) {
-                const unsigned long long tot = group_sum<32>(cur_sum, FULL);
+                const unsigned long long tot = group_sum<G>(cur_sum, gmask);
                 if (lane == 0 && tot) atomicAdd(p.sums + cur_key, tot);
                 cur_key = key;
                 cur_sum = 0;
@@ -198,11 +211,11 @@ __global__ void __launch_bounds__(NT, GK_LB_THREADS / NT) k_search(KArgs p) {
         }
     }
     if (EPI == EPI_KEYED && cur_key >= 0) {
-        const unsigned long long tot = group_sum<32>(cur_sum, FULL);
+        const unsigned long long tot = group_sum<G>(cur_sum, gmask);
         if (lane == 0 && tot) atomicAdd(p.sums + cur_key, tot);
     }
     if (EPI == EPI_SUM) {
-        const unsigned long long tot = group_sum<32>(local, FULL);
+        const unsigned long long tot = group_sum<G>(local, gmask);
         if (lane == 0 && tot) atomicAdd(p.sums, tot);
     }
 }

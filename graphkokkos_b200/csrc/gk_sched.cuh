@@ -48,7 +48,7 @@ struct Variant {
     int comp;       // block HASH kinds: filter candidates packed into a per-warp queue and checked one per lane
 };
 
-constexpr int NV = 22;
+constexpr int NV = 24;
 // Shared-memory budget of every variant is below 160 KB; see the kernels.
 // Tables are bucketed (four slots per 16-byte load).  The small ones run at
 // load factor <= 1/4 (chunk <= cap/4); the large ones of variants 6-8 and
@@ -67,7 +67,9 @@ constexpr int NV = 22;
 // hit then costs one bit test instead of a divergent table lookup.  Variants 20
 // and 21 are variants 8 and 15 with the filter candidates of a warp packed into
 // a shared-memory queue and checked one per lane (comp = 1), for rows whose
-// mask covers a large share of the streamed elements.
+// mask covers a large share of the streamed elements.  Variants 22 and 23 are
+// the search kind with half- and quarter-warps per row (two and four short
+// rows per warp).
 // columns: kind, G, sub, cap, cap (WRITE), chunk, chunk (WRITE), split_log2, filter log2, batch, accum, comp,
 // exact low-column bits (variants 15, 16: the filter maps columns below 2^lowb
 // one to one, so a hit there needs no table lookup when only sums are kept)
@@ -94,6 +96,8 @@ constexpr int NV = 22;
     {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 16, 1, 3  , 18, 0},  \
     {K_HASH_BLOCK, 512, 32, 16384, 16384,  8192,  8192,  20, 18, 1, 3  , 0, 1},  \
     {K_HASH_BLOCK, 512, 32,  8192, 16384,  4096,  8192,  20, 16, 1, 3  , 18, 1}, \
+    {K_SEARCH,      16, 16,    64,    64,    64,    64,   0,  0, 2, 0  , 0, 0},   \
+    {K_SEARCH,       8,  8,    32,    32,    32,    32,   0,  0, 2, 0  , 0, 0},   \
 }
 constexpr Variant VARIANTS[NV] = GK_VARIANT_TABLE;
 #ifdef __CUDACC__
@@ -133,6 +137,8 @@ __host__ __device__ constexpr bool variant_allowed(int v, int bin) {
         case 19: return qm >= 10;
         case 20:
         case 21: return qm >= 8;
+        case 22: return qm <= 6;
+        case 23: return qm <= 5;
         default: return false;
     }
 }

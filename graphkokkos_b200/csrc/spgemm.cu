@@ -13,7 +13,7 @@
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
 //                   get their item count (mask chunks x A-entry splits)
 //  5. one persistent kernel per variant over its rows / items (the catalogue
-//     of 22 variants is the table in gk_sched.cuh):
+//     of 24 variants is the table in gk_sched.cuh):
 //       HASH_GROUP  4, 8 or 32 threads per row, the mask row's columns in a
 //                   shared-memory bucketed hash set (slot = accumulator)
 //       MCA_GROUP   32 threads per row, mask row sorted in shared memory,
@@ -25,8 +25,9 @@
 //       MCA_BLOCK   one CTA per item, up to 16K sorted mask columns
 //       MSA_BLOCK   one CTA per item, dense column-window accumulator
 //                   (the reference's MSA, matrix_la.h:611-631) or bitmap
-//       SEARCH      a warp per row, each mask column inside B_k's column range
-//                   looked up in B_k by binary search (gk_ksearch.cuh)
+//       SEARCH      a warp (or half-/quarter-warp) per row, each mask column
+//                   inside B_k's column range looked up in B_k by binary
+//                   search (gk_ksearch.cuh)
 // B rows are streamed with 16-byte vector loads; mask chunks that do not cover
 // a whole mask row only stream the part of B_k inside the chunk's column range
 // (group-cooperative search).  Integer terms are summed in 32-bit wrapping
@@ -704,7 +705,7 @@ constexpr size_t smem_bytes(bool write) {
         const size_t stage_pad = (X.kind == K_MCA_GROUP) ? 16 : 0;  // cp.async alignment slots
         return size_t(ng) * (size_t(cap) * 4 * (write ? 2 : 1) + filter + stage_pad);
     } else if constexpr (X.kind == K_SEARCH) {
-        return size_t(NT_GROUP / 32) * size_t(write ? X.cap_write : X.cap) * 4 * (write ? 2 : 1);
+        return size_t(NT_GROUP / X.G) * size_t(write ? X.cap_write : X.cap) * 4 * (write ? 2 : 1);
     } else if constexpr (X.kind == K_MSA_BLOCK) {
         if (write) return (size_t(1) << X.cap_write) / 8 + (size_t(1) << X.cap_write) * 4;
         return (size_t(1) << X.cap) / 8;
@@ -734,7 +735,7 @@ static cudaError_t launch_variant_t(const KArgs &args, int num_sms, cudaStream_t
         fn = k_group<X.G, X.sub, NTV, CAPV, X.chunk, MCA, (MCA ? 0 : X.flog), EPI, VAL>;
         nt = NTV;
     } else if constexpr (X.kind == K_SEARCH) {
-        fn = k_search<NT_GROUP, (W ? X.cap_write : X.cap), EPI, VAL>;
+        fn = k_search<NT_GROUP, X.G, (W ? X.cap_write : X.cap), EPI, VAL>;
         nt = NT_GROUP;
     } else {
         constexpr int CAPV = W ? X.cap_write : X.cap;
@@ -795,6 +796,8 @@ static cudaError_t launch_variant(int v, const KArgs &a, int epi, bool val, int 
         case 19: return launch_variant_v<19>(a, epi, val, sms, s, launch);
         case 20: return launch_variant_v<20>(a, epi, val, sms, s, launch);
         case 21: return launch_variant_v<21>(a, epi, val, sms, s, launch);
+        case 22: return launch_variant_v<22>(a, epi, val, sms, s, launch);
+        case 23: return launch_variant_v<23>(a, epi, val, sms, s, launch);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -822,7 +825,7 @@ static const char *const kVariantRange[NV] = {
     "gk:variant 0",  "gk:variant 1",  "gk:variant 2",  "gk:variant 3",  "gk:variant 4",  "gk:variant 5",
     "gk:variant 6",  "gk:variant 7",  "gk:variant 8",  "gk:variant 9",  "gk:variant 10", "gk:variant 11",
     "gk:variant 12", "gk:variant 13", "gk:variant 14", "gk:variant 15", "gk:variant 16", "gk:variant 17",
-    "gk:variant 18", "gk:variant 19", "gk:variant 20", "gk:variant 21"};
+    "gk:variant 18", "gk:variant 19", "gk:variant 20", "gk:variant 21", "gk:variant 22", "gk:variant 23"};
 
 // ---------------------------------------------------------------------------
 // driver

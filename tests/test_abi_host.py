@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol(gk):
 
 def test_scheduler_shape(gk):
     lib = gk.load()
-    assert lib.gk_sched_num_variants() == 22
+    assert lib.gk_sched_num_variants() == 24
     assert lib.gk_sched_num_features() == 8
     assert lib.gk_sched_model_size() > 0
     assert lib.gk_version() >= 100

@@ -15,7 +15,7 @@ from tests import graphs as G
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-NV = 22
+NV = 24
 
 
 def dev(csr):
