@@ -162,35 +162,27 @@ __global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_
                         P[h].lo = 0;
                         P[h].len = P[h].live ? blen_j : 1;
                     }
-                    // narrow each pair's B row down to a window of at most
-                    // four entries that holds the last position with
-                    // B.col <= c (row[0] <= c holds: c lies inside the row's
-                    // range) ...
-                    while (P[0].len > 4 || P[1].len > 4) {
+                    // last position with B.col <= c in each pair's B row
+                    // (row[0] <= c holds: c lies inside the row's range)
+                    while (P[0].len > 1 || P[1].len > 1) {
                         int x[2];
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
-                            if (P[h].len > 4) x[h] = __ldg(P[h].row + P[h].lo + (P[h].len >> 1));
+                            if (P[h].len > 1) x[h] = __ldg(P[h].row + P[h].lo + (P[h].len >> 1));
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
-                            if (P[h].len > 4) {
+                            if (P[h].len > 1) {
                                 const int half = P[h].len >> 1;
                                 if (x[h] <= P[h].c) P[h].lo += half;
                                 P[h].len -= half;
                             }
                     }
-                    // ... and compare the window's entries with independent
-                    // loads instead of two more dependent halving steps
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        int hit = -1;
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                            if (P[h].live && e < P[h].len && __ldg(P[h].row + P[h].lo + e) == P[h].c) hit = P[h].lo + e;
-                        if (hit >= 0) {
+                        if (P[h].live && __ldg(P[h].row + P[h].lo) == P[h].c) {
                             const uint32_t w =
                                 (VAL && p.B.val)
-                                    ? P[h].av * static_cast<uint32_t>(__ldg(p.B.val + (P[h].row - p.B.col) + hit))
+                                    ? P[h].av * static_cast<uint32_t>(__ldg(p.B.val + (P[h].row - p.B.col) + P[h].lo))
                                     : P[h].av;
                             if (ACC) atomicAdd(reinterpret_cast<unsigned *>(acc + P[h].q), w);
                             else cnt += w;
