@@ -361,24 +361,28 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_pull(DevCsr AT, DevCsr A
     add_level_stats(n, e, b, &st->nn);
 }
 
-// Reduces the NW warps' T x 32 partial sums of a CTA into warp 0's acc.
+// Sums the NW warps' T x 32 partial sums of a CTA (each warp accumulated into
+// its own slice of part) into dst[32 t + lane], in warp order.
 template <int T>
-__device__ __forceinline__ void cta_reduce(double (&acc)[T], double (*part)[T][32], int warp, int lane) {
-#pragma unroll
-    for (int t = 0; t < T; ++t) part[warp][t][lane] = acc[t];
+__device__ __forceinline__ void cta_reduce_store(double (*part)[T][32], int warp, int lane, double *dst) {
     __syncthreads();
     if (warp == 0) {
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             double sum = 0.0;
             for (int w = 0; w < BC_NW_HEAVY; ++w) sum += part[w][t][lane];
-            acc[t] = sum;
+            dst[32 * t + lane] = sum;
         }
     }
 }
 
+// Resident CTAs per SM of the heavy-vertex item kernels: their per-lane
+// partial sums live in the CTA's reduction buffer (shared memory), not in
+// registers, so four 8-warp CTAs fit (64 registers a thread).
+constexpr int BC_ITEM_MINB = 4;
+
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_items(DevCsr AT, HeavySet hs, BcState *st,
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_pull_items(DevCsr AT, HeavySet hs, BcState *st,
                                                                     const uint32_t *V, const double *sigma, int W,
                                                                     const uint32_t *act, double *partials) {
     if (st->mode != BC_PULL) return;
@@ -399,15 +403,11 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_pull_items(DevCsr AT, H
             open |= need[t];
         }
         if (!open) continue;  // uniform across the CTA (the emit kernel skips the vertex too)
-        double acc[T];
+        SmemAcc acc{&part[warp][0][lane]};
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
         pull_sigma<T>(AT, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fd, need, sigma, W, lane, acc);
-        cta_reduce<T>(acc, part, warp, lane);
-        if (warp == 0) {
-#pragma unroll
-            for (int t = 0; t < T; ++t) partials[(int64_t)it * W + 32 * t + lane] = acc[t];
-        }
+        cta_reduce_store<T>(part, warp, lane, partials + (int64_t)it * W);
         __syncthreads();
     }
 }
@@ -682,7 +682,8 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
 }
 
 template <int T>
-__global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_items(DevCsr A, HeavySet hs, const BcState *st,
+__global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_backward_items(DevCsr A, HeavySet hs,
+                                                                                     const BcState *st,
                                                                         const double *R, int W, double *partials) {
     __shared__ double part[BC_NW_HEAVY][T][32];
     const int d = st->bd;
@@ -700,15 +701,11 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_backward_items(DevCsr A
 #pragma unroll
         for (int t = 0; t < T; ++t) any |= fv[t];
         if (!any) continue;
-        double sum[T];
+        SmemAcc sum{&part[warp][0][lane]};
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
         pull_r<T>(A, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
-        cta_reduce<T>(sum, part, warp, lane);
-        if (warp == 0) {
-#pragma unroll
-            for (int t = 0; t < T; ++t) partials[(int64_t)it * W + 32 * t + lane] = sum[t];
-        }
+        cta_reduce_store<T>(part, warp, lane, partials + (int64_t)it * W);
         __syncthreads();
     }
 }
@@ -932,7 +929,8 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
             k_bc_pull<T><<<sms * 8, 256, 0, ls>>>(g.AT, g.A, st, V, sigma, W, act);
             int k = 0;
             if (g.hAT.n) {
-                k_bc_pull_items<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.AT, g.hAT, st, V, sigma, W, act, partials);
+                k_bc_pull_items<T><<<sms * BC_ITEM_MINB, BC_NW_HEAVY * 32, 0, ls>>>(g.AT, g.hAT, st, V, sigma, W, act,
+                                                                                   partials);
                 k_bc_pull_heavy_emit<T><<<sms, 256, 0, ls>>>(g.A, g.hAT, st, V, sigma, W, act, partials);
                 k += 2;
             }
@@ -1031,7 +1029,7 @@ static int bc_chunk(const BcBuffers &g, const int32_t *src, int nsrc, double *bc
             k_bc_backward<T><<<sms * 8, 256, 0, ls>>>(g.A, st, sigma, R, W, bc);
             int k = 0;
             if (g.hA.n) {
-                k_bc_backward_items<T><<<sms * 2, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.hA, st, R, W, partials);
+                k_bc_backward_items<T><<<sms * BC_ITEM_MINB, BC_NW_HEAVY * 32, 0, ls>>>(g.A, g.hA, st, R, W, partials);
                 k_bc_backward_heavy_emit<T><<<sms, 256, 0, ls>>>(g.hA, st, sigma, R, W, bc, partials);
                 k += 2;
             }
