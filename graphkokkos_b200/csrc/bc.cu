@@ -16,8 +16,9 @@
 //   visited bitmap V[v*T + t]
 // Forward levels run one of two kernel shapes, chosen per level on the device:
 //   pull  one warp per vertex with sources still open: its lanes test 32
-//         in-neighbours' frontier words at a time, then for each neighbour that
-//         carries a needed bit the lanes (one per source) add sigma;
+//         in-neighbours' frontier words at a time, then take the (neighbour,
+//         source) hits 32 at a time, one per lane, each adding the neighbour's
+//         sigma of its source into the vertex's sum of that source;
 //   push  one warp per frontier vertex: its lanes test 32 out-neighbours'
 //         visited words at a time, then add sigma into the new vertices with
 //         FP64 atomics.  sigma are path counts, integers below 2^53 in FP64, so
@@ -26,7 +27,8 @@
 // edges still to explore (Beamer's direction-optimising rule); the learned
 // rule is an MLP over the level's frontier statistics, trained on measured
 // per-level times of both shapes.  Backward levels pull: one warp per vertex
-// of level d, lanes testing 32 successors' level-(d+1) words at a time.
+// of level d, lanes testing 32 successors' level-(d+1) words at a time and
+// gathering their R words hit by hit in the same way.
 // Vertices with more than BC_HEAVY neighbours have their neighbour lists cut
 // into items of BC_ITEM_EDGES edges, one CTA each, so that a hub no longer
 // holds one CTA for the whole level; the items' partial sums are added per
@@ -143,6 +145,8 @@ __device__ __forceinline__ void load_words_rw(const uint32_t *p, uint32_t (&w)[T
 struct SmemAcc {
     double *p;
     __device__ __forceinline__ double &operator[](int t) const { return p[32 * t]; }
+    // the warp's slice, source s at [s]
+    __device__ __forceinline__ double *warp_base(int lane) const { return p - lane; }
 };
 
 // One atomic per block and counter.
@@ -264,39 +268,137 @@ __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_
 // ---------------------------------------------------------------------------
 // forward, pull: in-neighbours (AT) of a vertex with open sources
 // ---------------------------------------------------------------------------
-// Lanes test 32 neighbours' frontier words at a time; each neighbour carrying
-// a needed bit then has its sigma words added by the lanes of those sources.
-template <int T, class AccT>
-__device__ __forceinline__ bool pull_sigma(const DevCsr &AT, int64_t ebeg, int64_t e1, int64_t estep,
-                                           const uint32_t *__restrict__ Fd, const uint32_t (&need)[T],
-                                           const double *__restrict__ sigma, int W, int lane, AccT &acc) {
+// Copies the warp's T selection words (equal in every lane) to its slot in
+// shared memory, so that they take no registers through a gather.
+template <int T>
+__device__ __forceinline__ const uint32_t *stage_sel(uint32_t *slot, const uint32_t (&x)[T], int lane) {
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < T; ++t)
+        if (lane == t) slot[t] = x[t];
+    __syncwarp();
+    return slot;
+}
+
+// Position of the k-th set bit (from 0) of x, which has more than k set bits.
+__device__ __forceinline__ int nth_set_bit(uint32_t x, int k) {
+    int p = 0;
+    int c = __popc(x & 0xFFFFu);
+    if (k >= c) { k -= c; x >>= 16; p += 16; }
+    c = __popc(x & 0xFFu);
+    if (k >= c) { k -= c; x >>= 8; p += 8; }
+    c = __popc(x & 0xFu);
+    if (k >= c) { k -= c; x >>= 4; p += 4; }
+    c = __popc(x & 0x3u);
+    if (k >= c) { k -= c; x >>= 2; p += 2; }
+    if (k >= static_cast<int>(x & 1u)) p += 1;
+    return p;
+}
+
+// Pull gather over the edges [ebeg, e1) of one vertex, 32 edges per warp step
+// (estep between a warp's steps).  The edge to neighbour w = G.col[e] carries
+// the hits F[w][t] & sel[t] (sel: the warp's T words in shared memory): source s = 32 t + l hits when bit l of that word
+// is set, and each hit adds a_e * X[w W + s] into the warp's accumulator of
+// source s (acc: the warp's T x 32 slice in shared memory, source s at s).
+// Where a step's hits are sparse (at most 32 per hit edge on average) they are
+// numbered in (edge, word, bit) order and taken 32 at a time, one per lane, so
+// that a load instruction carries 32 hits however few sources each (edge,
+// word) holds (typically 1.5 to 6 of 32), and the step costs one load latency
+// per 32 hits instead of one per hit edge.  Every source's sum is taken in
+// edge order: the hits of one source within a batch belong to different edges
+// and are applied in lane order.  Returns whether any edge hit (the same in
+// every lane).
+template <int T>
+__device__ __forceinline__ bool pull_gather(const DevCsr &G, int64_t ebeg, int64_t e1, int64_t estep,
+                                            const uint32_t *__restrict__ F, const uint32_t *sel,
+                                            const double *__restrict__ X, int W, int lane, double *acc) {
+    constexpr unsigned FULL = 0xFFFFFFFFu;
     bool any = false;
     for (int64_t base = ebeg; base < e1; base += estep) {
         const int64_t e = base + lane;
-        int u = 0;
-        uint32_t hitw = 0;
-        if (e < e1) {
-            u = __ldg(AT.col + e);
-            uint32_t f[T];
-            load_words<T>(Fd + (int64_t)u * T, f);
+        int w = 0;
+        uint32_t h[T];
 #pragma unroll
-            for (int t = 0; t < T; ++t) hitw |= f[t] & need[t];
+        for (int t = 0; t < T; ++t) h[t] = 0u;
+        if (e < e1) {
+            w = __ldg(G.col + e);
+            load_words<T>(F + (int64_t)w * T, h);
+#pragma unroll
+            for (int t = 0; t < T; ++t) h[t] &= sel[t];
         }
-        unsigned bal = __ballot_sync(0xFFFFFFFFu, hitw != 0);
-        if (bal) any = true;
-        while (bal) {
-            const int j = __ffs(bal) - 1;
-            bal &= bal - 1;
-            const int uu = __shfl_sync(0xFFFFFFFFu, u, j);
-            const double a = AT.val ? static_cast<double>(__ldg(AT.val + base + j)) : 1.0;
-            uint32_t f[T];
-            load_words<T>(Fd + (int64_t)uu * T, f);
-            const double *__restrict__ su = sigma + (int64_t)uu * W + lane;
+        int c = 0;
+#pragma unroll
+        for (int t = 0; t < T; ++t) c += __popc(h[t]);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int n = __shfl_sync(FULL, incl, 31);
+        if (n) any = true;
+        const unsigned edges = __ballot_sync(FULL, c > 0);
+        if (n > 32 * __popc(edges)) {
+            // dense hits (more than 32 per hit edge, as at a hub's middle
+            // levels): one edge at a time, a load per word, no worse than a
+            // batch of 32 in lanes used and with fewer instructions per hit
+            for (unsigned bal = edges; bal; bal &= bal - 1) {
+                const int j = __ffs(bal) - 1;
+                const int wj = __shfl_sync(FULL, w, j);
+                const double a = G.val ? static_cast<double>(__ldg(G.val + base + j)) : 1.0;
+                const double *__restrict__ xw = X + (int64_t)wj * W + lane;
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    const uint32_t bits = __shfl_sync(FULL, h[t], j);
+                    if ((bits >> lane) & 1u) acc[32 * t + lane] += a * __ldg(xw + 32 * t);
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        const int excl = incl - c;
+        for (int q0 = 0; q0 < n; q0 += 32) {
+            const int q = q0 + lane;
+            // j = the lane (edge) holding hit q: lanes below j end at or before q
+            int j = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (__shfl_sync(FULL, incl, j + step - 1) <= q) j += step;
+            int r = q - __shfl_sync(FULL, excl, j);
+            const int wj = __shfl_sync(FULL, w, j);
+            uint32_t word = 0u;
+            int tt = 0, rk = 0;
 #pragma unroll
             for (int t = 0; t < T; ++t) {
-                const uint32_t bits = f[t] & need[t];
-                if (bits && ((bits >> lane) & 1u)) acc[t] += a * __ldg(su + 32 * t);
+                const uint32_t x = __shfl_sync(FULL, h[t], j);
+                const int p = __popc(x);
+                if (r >= 0 && r < p) {
+                    word = x;
+                    tt = t;
+                    rk = r;
+                }
+                r -= p;
             }
+            const bool ok = q < n;
+            const int s = 32 * tt + nth_set_bit(word, rk);
+            double v = 0.0, a = 1.0;
+            if (ok) {
+                v = __ldg(X + (int64_t)wj * W + s);
+                if (G.val) a = static_cast<double>(__ldg(G.val + base + j));
+            }
+            const int jlast = __shfl_sync(FULL, j, min(n - q0, 32) - 1);
+            if (__shfl_sync(FULL, j, 0) == jlast) {
+                if (ok) acc[s] += a * v;  // one edge: distinct sources
+            } else {
+                const unsigned same = __match_any_sync(FULL, ok ? static_cast<unsigned>(s) : W + lane);
+                const unsigned rank = __popc(same & ((1u << lane) - 1u));
+                const unsigned rounds = __reduce_max_sync(FULL, ok ? rank : 0u);
+                for (unsigned k = 0; k <= rounds; ++k) {
+                    if (ok && rank == k) acc[s] += a * v;
+                    __syncwarp();
+                }
+            }
+            __syncwarp();
         }
     }
     return any;
@@ -333,6 +435,7 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_pull(DevCsr AT, DevCsr A
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
     __shared__ double s_acc[8][T][32];
+    __shared__ uint32_t s_sel[8][T];
     SmemAcc acc{&s_acc[threadIdx.x >> 5][0][lane]};
     unsigned long long n = 0, e = 0, b = 0;
     for (int64_t base = grab_vertices(&st->cur_pull, lane); base < AT.m; base = grab_vertices(&st->cur_pull, lane))
@@ -350,7 +453,8 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_pull(DevCsr AT, DevCsr A
         if (!open) continue;
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
-        if (!pull_sigma<T>(AT, e0, e1, 32, Fd, need, sigma, W, lane, acc)) continue;
+        const uint32_t *sel = stage_sel<T>(s_sel[threadIdx.x >> 5], need, lane);
+        if (!pull_gather<T>(AT, e0, e1, 32, Fd, sel, sigma, W, lane, acc.warp_base(lane))) continue;
         const int c = pull_emit<T>(i, W, lane, acc, Fn, V, sigma);
         if (c && lane == 0) {
             ++n;
@@ -387,6 +491,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_pull_item
                                                                     const uint32_t *act, double *partials) {
     if (st->mode != BC_PULL) return;
     __shared__ double part[BC_NW_HEAVY][T][32];
+    __shared__ uint32_t s_sel[BC_NW_HEAVY][T];
     const uint32_t *__restrict__ Fd = st->fptr[st->d];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
@@ -406,7 +511,8 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_pull_item
         SmemAcc acc{&part[warp][0][lane]};
 #pragma unroll
         for (int t = 0; t < T; ++t) acc[t] = 0.0;
-        pull_sigma<T>(AT, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fd, need, sigma, W, lane, acc);
+        const uint32_t *sel = stage_sel<T>(s_sel[warp], need, lane);
+        pull_gather<T>(AT, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fd, sel, sigma, W, lane, acc.warp_base(lane));
         cta_reduce_store<T>(part, warp, lane, partials + (int64_t)it * W);
         __syncthreads();
     }
@@ -604,39 +710,6 @@ __global__ void k_bc_rinit(int64_t m, const BcState *st, const double *sigma, do
 }
 
 template <int T, class AccT>
-__device__ __forceinline__ void pull_r(const DevCsr &A, int64_t ebeg, int64_t e1, int64_t estep,
-                                       const uint32_t *__restrict__ Fn, const uint32_t (&fv)[T],
-                                       const double *__restrict__ R, int W, int lane, AccT &sum) {
-    for (int64_t base = ebeg; base < e1; base += estep) {
-        const int64_t e = base + lane;
-        int w = 0;
-        uint32_t hitw = 0;
-        if (e < e1) {
-            w = __ldg(A.col + e);
-            uint32_t f[T];
-            load_words<T>(Fn + (int64_t)w * T, f);
-#pragma unroll
-            for (int t = 0; t < T; ++t) hitw |= f[t] & fv[t];
-        }
-        unsigned bal = __ballot_sync(0xFFFFFFFFu, hitw != 0);
-        while (bal) {
-            const int j = __ffs(bal) - 1;
-            bal &= bal - 1;
-            const int ww = __shfl_sync(0xFFFFFFFFu, w, j);
-            const double a = A.val ? static_cast<double>(__ldg(A.val + base + j)) : 1.0;
-            uint32_t f[T];
-            load_words<T>(Fn + (int64_t)ww * T, f);
-            const double *__restrict__ rw = R + (int64_t)ww * W + lane;
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const uint32_t bits = f[t] & fv[t];
-                if (bits && ((bits >> lane) & 1u)) sum[t] += a * __ldg(rw + 32 * t);
-            }
-        }
-    }
-}
-
-template <int T, class AccT>
 __device__ __forceinline__ void bwd_emit(int64_t v, int W, int lane, const uint32_t (&fv)[T], const AccT &sum,
                                          const double *sigma, double *R, double *bc) {
     double tot = 0.0;
@@ -663,6 +736,7 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31;
     __shared__ double s_sum[8][T][32];
+    __shared__ uint32_t s_sel[8][T];
     SmemAcc sum{&s_sum[threadIdx.x >> 5][0][lane]};
     for (int64_t base = grab_vertices(&st->cur_bwd, lane); base < A.m; base = grab_vertices(&st->cur_bwd, lane))
     for (int64_t v = base, vend = min(base + BC_GRAB, A.m); v < vend; ++v) {
@@ -676,7 +750,10 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
         if (!any) continue;
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
-        pull_r<T>(A, e0, e1, 32, Fn, fv, R, W, lane, sum);
+        const uint32_t *sel = stage_sel<T>(s_sel[threadIdx.x >> 5], fv, lane);
+        pull_gather<T>(A, e0, e1, 32, Fn, sel, R, W, lane, sum.warp_base(lane));
+#pragma unroll
+        for (int t = 0; t < T; ++t) fv[t] = sel[t];
         bwd_emit<T>(v, W, lane, fv, sum, sigma, R, bc);
     }
 }
@@ -686,6 +763,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_backward_
                                                                                      const BcState *st,
                                                                         const double *R, int W, double *partials) {
     __shared__ double part[BC_NW_HEAVY][T][32];
+    __shared__ uint32_t s_sel[BC_NW_HEAVY][T];
     const int d = st->bd;
     const uint32_t *__restrict__ Fd = st->fptr[d];
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
@@ -704,7 +782,8 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_backward_
         SmemAcc sum{&part[warp][0][lane]};
 #pragma unroll
         for (int t = 0; t < T; ++t) sum[t] = 0.0;
-        pull_r<T>(A, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fn, fv, R, W, lane, sum);
+        const uint32_t *sel = stage_sel<T>(s_sel[warp], fv, lane);
+        pull_gather<T>(A, e0 + 32 * warp, e1, 32 * BC_NW_HEAVY, Fn, sel, R, W, lane, sum.warp_base(lane));
         cta_reduce_store<T>(part, warp, lane, partials + (int64_t)it * W);
         __syncthreads();
     }

@@ -458,7 +458,7 @@ SideStreams &side_streams() {
     dev &= 15;
     if (!ready[dev]) {
         SideStreams &x = per_dev[dev];
-        for (int i = 0; i < 16; ++i) {
+        for (int i = 0; i < kSideStreams; ++i) {
             cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking);
             cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming);
         }

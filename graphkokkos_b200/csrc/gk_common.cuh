@@ -118,10 +118,11 @@ inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) 
 // ----- side streams for concurrent kernel variants ----------------------------
 // Non-blocking streams and fork/join events, one set per host thread and
 // device, so that concurrent callers never share an event.
+constexpr int kSideStreams = 32;  // at least the number of kernel variants
 struct SideStreams {
-    cudaStream_t s[16];
+    cudaStream_t s[kSideStreams];
     cudaEvent_t fork;
-    cudaEvent_t join[16];
+    cudaEvent_t join[kSideStreams];
 };
 SideStreams &side_streams();
 

@@ -920,6 +920,7 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
         const char *e = getenv("GK_CONCURRENT_VARIANTS");
         return e && e[0] == '1';
     }();
+    static_assert(NV <= kSideStreams, "one side stream per variant");
     SideStreams &side = side_streams();
     const bool fork = concurrent && rq.force_variant < 0;
     if (fork) GK_CUDA(cudaEventRecord(side.fork, s));

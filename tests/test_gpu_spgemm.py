@@ -77,6 +77,24 @@ def test_tc_rmat18(gk, orc, cuda):
         assert gk.tc_count_variant(L, v) == want
 
 
+def test_tc_concurrent_variant_streams(gk, orc, cuda):
+    """GK_CONCURRENT_VARIANTS=1 forks every variant kernel onto its own side
+    stream (the library reads the setting once per process, so the check runs
+    in a child process): same counts under both schedulers."""
+    import subprocess
+    import sys
+    A = gk.gen_rmat(16, 16, seed=2)
+    want = orc.tc_lower(gk.lower_host(A))
+    code = ("import graphkokkos_b200 as gk; from graphkokkos_b200 import sched; sched.load_model(); "
+            "L = gk.extract_lower(gk.gen_rmat(16, 16, seed=2, device='cuda')); "
+            "print(gk.tc_count(L, sched='plain'), gk.tc_count(L, sched='learned'))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, GK_CONCURRENT_VARIANTS="1"))
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.split() == [str(want), str(want)]
+
+
 def test_tc_row_sums(gk, orc, cuda):
     A = gk.gen_rmat(12, 16, seed=8)
     L = gk.lower_host(A)
