@@ -65,6 +65,11 @@ namespace gk {
 #ifndef GK_BC_MINB
 #define GK_BC_MINB 4
 #endif
+// A gather step whose hits average more than this per hit edge takes its
+// edges one at a time (see pull_gather).
+#ifndef GK_BC_DENSE_HITS
+#define GK_BC_DENSE_HITS 32
+#endif
 constexpr int BC_HEAVY = 512;
 constexpr int BC_NW_HEAVY = 8;  // T=16: 8*16*32 doubles = 32 KB of static shared memory
 constexpr int BC_PULL = 0, BC_PUSH = 1;
@@ -108,7 +113,10 @@ struct BcState {
 
 // Light kernels hand vertices to warps BC_GRAB at a time from a counter, so
 // that a warp which met expensive vertices does not hold the level back.
-constexpr int BC_GRAB = 16;
+#ifndef GK_BC_GRAB
+#define GK_BC_GRAB 2
+#endif
+constexpr int BC_GRAB = GK_BC_GRAB;
 __device__ __forceinline__ int64_t grab_vertices(unsigned long long *cursor, int lane) {
     unsigned long long b = 0;
     if (lane == 0) b = atomicAdd(cursor, static_cast<unsigned long long>(BC_GRAB));
@@ -300,11 +308,11 @@ __device__ __forceinline__ int nth_set_bit(uint32_t x, int k) {
 // the hits F[w][t] & sel[t] (sel: the warp's T words in shared memory): source s = 32 t + l hits when bit l of that word
 // is set, and each hit adds a_e * X[w W + s] into the warp's accumulator of
 // source s (acc: the warp's T x 32 slice in shared memory, source s at s).
-// Where a step's hits are sparse (at most 32 per hit edge on average) they are
-// numbered in (edge, word, bit) order and taken 32 at a time, one per lane, so
-// that a load instruction carries 32 hits however few sources each (edge,
-// word) holds (typically 1.5 to 6 of 32), and the step costs one load latency
-// per 32 hits instead of one per hit edge.  Every source's sum is taken in
+// Where a step's hits are sparse (at most GK_BC_DENSE_HITS per hit edge on
+// average) they are numbered in (edge, word, bit) order and taken 32 at a
+// time, one per lane, so that a load instruction carries 32 hits however few
+// sources each (edge, word) holds (typically 1.5 to 6 of 32), and the step
+// costs one load latency per 32 hits instead of one per hit edge.  Every source's sum is taken in
 // edge order: the hits of one source within a batch belong to different edges
 // and are applied in lane order.  Returns whether any edge hit (the same in
 // every lane).
@@ -338,7 +346,7 @@ __device__ __forceinline__ bool pull_gather(const DevCsr &G, int64_t ebeg, int64
         const int n = __shfl_sync(FULL, incl, 31);
         if (n) any = true;
         const unsigned edges = __ballot_sync(FULL, c > 0);
-        if (n > 32 * __popc(edges)) {
+        if (n > GK_BC_DENSE_HITS * __popc(edges)) {
             // dense hits (more than 32 per hit edge, as at a hub's middle
             // levels): one edge at a time, a load per word, no worse than a
             // batch of 32 in lanes used and with fewer instructions per hit
