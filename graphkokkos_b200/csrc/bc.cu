@@ -70,12 +70,18 @@ namespace gk {
 #ifndef GK_BC_DENSE_HITS
 #define GK_BC_DENSE_HITS 32
 #endif
-constexpr int BC_HEAVY = 512;
+#ifndef GK_BC_HEAVY
+#define GK_BC_HEAVY 512
+#endif
+#ifndef GK_BC_ITEM_EDGES
+#define GK_BC_ITEM_EDGES 1024
+#endif
+constexpr int BC_HEAVY = GK_BC_HEAVY;
 constexpr int BC_NW_HEAVY = 8;  // T=16: 8*16*32 doubles = 32 KB of static shared memory
 constexpr int BC_PULL = 0, BC_PUSH = 1;
 constexpr int BC_LEVEL_BATCH = 16;  // level bitmaps allocated at a time
 constexpr int BC_FEAT = NFEAT;
-constexpr int BC_ITEM_EDGES = 2048;  // edges of a heavy vertex per CTA work item
+constexpr int BC_ITEM_EDGES = GK_BC_ITEM_EDGES;  // edges of a heavy vertex per CTA work item
 
 // Vertices with more than BC_HEAVY neighbours, their neighbour lists cut
 // into items of BC_ITEM_EDGES edges (one CTA each).  Pull-type items write
@@ -109,6 +115,7 @@ struct BcState {
     unsigned long long visited;     // (vertex, source) pairs reached, sources included
     unsigned long long pushes, pulls;
     unsigned long long cur_pull, cur_push, cur_bwd;  // vertex cursors of the light kernels
+    unsigned long long cur_ipull, cur_ipush, cur_ibwd;  // item cursors of the heavy-vertex kernels
 };
 
 // Light kernels hand vertices to warps BC_GRAB at a time from a counter, so
@@ -121,6 +128,18 @@ __device__ __forceinline__ int64_t grab_vertices(unsigned long long *cursor, int
     unsigned long long b = 0;
     if (lane == 0) b = atomicAdd(cursor, static_cast<unsigned long long>(BC_GRAB));
     return static_cast<int64_t>(__shfl_sync(0xFFFFFFFFu, b, 0));
+}
+
+// The heavy-vertex item kernels take items one per CTA from a counter too:
+// items of one level differ in cost (their hit densities), so a fixed
+// round-robin share per CTA left the level waiting on the unluckiest CTA.
+// Every thread of the CTA calls it (it contains barriers).
+__device__ __forceinline__ int next_item(unsigned long long *cursor) {
+    __shared__ int s_item;
+    __syncthreads();  // the previous item's index has been read by all
+    if (threadIdx.x == 0) s_item = static_cast<int>(atomicAdd(cursor, 1ull));
+    __syncthreads();
+    return s_item;
 }
 
 template <int T>
@@ -305,17 +324,18 @@ __device__ __forceinline__ int nth_set_bit(uint32_t x, int k) {
 
 // Pull gather over the edges [ebeg, e1) of one vertex, 32 edges per warp step
 // (estep between a warp's steps).  The edge to neighbour w = G.col[e] carries
-// the hits F[w][t] & sel[t] (sel: the warp's T words in shared memory): source s = 32 t + l hits when bit l of that word
-// is set, and each hit adds a_e * X[w W + s] into the warp's accumulator of
-// source s (acc: the warp's T x 32 slice in shared memory, source s at s).
-// Where a step's hits are sparse (at most GK_BC_DENSE_HITS per hit edge on
-// average) they are numbered in (edge, word, bit) order and taken 32 at a
-// time, one per lane, so that a load instruction carries 32 hits however few
-// sources each (edge, word) holds (typically 1.5 to 6 of 32), and the step
-// costs one load latency per 32 hits instead of one per hit edge.  Every source's sum is taken in
-// edge order: the hits of one source within a batch belong to different edges
-// and are applied in lane order.  Returns whether any edge hit (the same in
-// every lane).
+// the hits F[w][t] & sel[t] (sel: the warp's T words in shared memory): source
+// s = 32 t + l hits when bit l of that word is set, and each hit adds
+// a_e * X[w W + s] into the warp's accumulator of source s (acc: the warp's
+// T x 32 slice in shared memory, source s at s).  Where a step's hits are
+// sparse (at most GK_BC_DENSE_HITS per hit edge on average) they are numbered
+// in (edge, word, bit) order and taken 32 at a time, one per lane, so that a
+// load instruction carries 32 hits however few sources each (edge, word)
+// holds (typically 1.5 to 6 of 32), and the step costs one load latency per
+// 32 hits instead of one per hit edge.  Every source's sum is taken in edge
+// order: the hits of one source within a batch belong to different edges and
+// are applied in lane order.  Returns whether any edge hit (the same in every
+// lane).
 template <int T>
 __device__ __forceinline__ bool pull_gather(const DevCsr &G, int64_t ebeg, int64_t e1, int64_t estep,
                                             const uint32_t *__restrict__ F, const uint32_t *sel,
@@ -347,9 +367,9 @@ __device__ __forceinline__ bool pull_gather(const DevCsr &G, int64_t ebeg, int64
         if (n) any = true;
         const unsigned edges = __ballot_sync(FULL, c > 0);
         if (n > GK_BC_DENSE_HITS * __popc(edges)) {
-            // dense hits (more than 32 per hit edge, as at a hub's middle
-            // levels): one edge at a time, a load per word, no worse than a
-            // batch of 32 in lanes used and with fewer instructions per hit
+            // dense hits (more than GK_BC_DENSE_HITS per hit edge, as at a
+            // hub's middle levels): one edge at a time, one load per source
+            // word, each carrying many hits, without the per-hit search
             for (unsigned bal = edges; bal; bal &= bal - 1) {
                 const int j = __ffs(bal) - 1;
                 const int wj = __shfl_sync(FULL, w, j);
@@ -502,7 +522,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_pull_item
     __shared__ uint32_t s_sel[BC_NW_HEAVY][T];
     const uint32_t *__restrict__ Fd = st->fptr[st->d];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+    for (int it = next_item(&st->cur_ipull); it < hs.items; it = next_item(&st->cur_ipull)) {
         const int h = hs.item_h[it];
         const int64_t i = hs.list[h];
         const int64_t e0 = AT.rp[i] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
@@ -643,7 +663,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32) k_bc_push_items(DevCsr A, He
     const uint32_t *__restrict__ Fd = st->fptr[d];
     uint32_t *Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+    for (int it = next_item(&st->cur_ipush); it < hs.items; it = next_item(&st->cur_ipush)) {
         const int h = hs.item_h[it];
         const int64_t u = hs.list[h];
         const int64_t e0 = A.rp[u] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
@@ -696,6 +716,7 @@ __global__ void k_bc_fwd_end(BcState *st, int64_t max_depth, cudaGraphConditiona
     }
     st->nn = st->en = st->bn = 0;
     st->cur_pull = st->cur_push = 0;
+    st->cur_ipull = st->cur_ipush = 0;
     if (in_graph) cudaGraphSetConditional(h, static_cast<unsigned>(more));
 }
 
@@ -768,7 +789,7 @@ __global__ void __launch_bounds__(256, GK_BC_MINB) k_bc_backward(DevCsr A, BcSta
 
 template <int T>
 __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_backward_items(DevCsr A, HeavySet hs,
-                                                                                     const BcState *st,
+                                                                                     BcState *st,
                                                                         const double *R, int W, double *partials) {
     __shared__ double part[BC_NW_HEAVY][T][32];
     __shared__ uint32_t s_sel[BC_NW_HEAVY][T];
@@ -776,7 +797,7 @@ __global__ void __launch_bounds__(BC_NW_HEAVY * 32, BC_ITEM_MINB) k_bc_backward_
     const uint32_t *__restrict__ Fd = st->fptr[d];
     const uint32_t *__restrict__ Fn = st->fptr[d + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int it = blockIdx.x; it < hs.items; it += gridDim.x) {
+    for (int it = next_item(&st->cur_ibwd); it < hs.items; it = next_item(&st->cur_ibwd)) {
         const int h = hs.item_h[it];
         const int64_t v = hs.list[h];
         const int64_t e0 = A.rp[v] + static_cast<int64_t>(it - hs.first[h]) * BC_ITEM_EDGES;
@@ -826,6 +847,7 @@ __global__ void __launch_bounds__(256) k_bc_backward_heavy_emit(HeavySet hs, con
 __global__ void k_bc_bwd_end(BcState *st, cudaGraphConditionalHandle h, int in_graph) {
     st->bd -= 1;
     st->cur_bwd = 0;
+    st->cur_ibwd = 0;
     if (in_graph) cudaGraphSetConditional(h, st->bd >= 1 ? 1u : 0u);
 }
 
