@@ -62,49 +62,84 @@ struct KArgs {
 // ---------------------------------------------------------------------------
 // plan kernels
 // ---------------------------------------------------------------------------
-__global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < A.m; r += warps) {
-        const int64_t a0 = A.rp[r], a1 = A.rp[r + 1];
-        long long w = 0;
-        int mb = 0;
-        int64_t t = a0 + lane;
-        // eight independent column / row-pointer load pairs in flight per lane:
-        // a hub row (10^5 entries) is one warp's loop, and its length in
-        // dependent load latencies bounds the kernel
-        constexpr int U = 8;
-        for (; t + 32 * (U - 1) < a1; t += 32 * U) {
-            int k[U];
+// Per row r of A: work[r] = sum of the B-row lengths of its entries, maxb[r] =
+// the longest of them.  Eight lanes per row, four rows per warp step (most rows
+// have a few dozen entries, so a warp per row left most lanes idle through its
+// dependent loads); a row of up to 32 entries is one dependent load chain of
+// its eight lanes.  Rows longer than ROW_STATS_LONG entries are taken by the
+// whole warp afterwards, eight independent load pairs in flight per lane, so
+// that a hub row (10^5 entries) is one warp's loop.
+constexpr int ROW_STATS_LONG = 256;
+
+// Entries t, t + step, ... < a1 of a row, U of them per lane in flight at a
+// time: the U column loads, then the U row-pointer pairs they name, so that a
+// row of at most step * U entries costs one dependent load chain.
+template <int U>
+__device__ __forceinline__ void row_stats_entries(const DevCsr &A, const DevCsr &B, int64_t t, int64_t a1, int step,
+                                                  long long &w, int &mb) {
+    for (; t < a1; t += static_cast<int64_t>(step) * U) {
+        int k[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) k[u] = __ldg(A.col + t + 32 * u);
-            int64_t b0[U], b1[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                b0[u] = __ldg(B.rp + k[u]);
-                b1[u] = __ldg(B.rp + k[u] + 1);
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int len = static_cast<int>(b1[u] - b0[u]);
-                w += len;
-                mb = max(mb, len);
-            }
+        for (int u = 0; u < U; ++u) {
+            const int64_t q = t + static_cast<int64_t>(step) * u;
+            k[u] = q < a1 ? __ldg(A.col + q) : -1;
         }
-        for (; t < a1; t += 32) {
-            const int k = __ldg(A.col + t);
-            const int len = static_cast<int>(__ldg(B.rp + k + 1) - __ldg(B.rp + k));
+        int64_t b0[U], b1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            b0[u] = k[u] >= 0 ? __ldg(B.rp + k[u]) : 0;
+            b1[u] = k[u] >= 0 ? __ldg(B.rp + k[u] + 1) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int len = static_cast<int>(b1[u] - b0[u]);
             w += len;
             mb = max(mb, len);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            w += __shfl_xor_sync(0xFFFFFFFFu, w, o);
-            mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+    }
+}
+
+__global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, sl = lane & 7;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < A.m; base += warps * 4) {
+        const int64_t r = base + (lane >> 3);
+        int64_t a0 = 0, a1 = 0;
+        if (r < A.m) {
+            a0 = A.rp[r];
+            a1 = A.rp[r + 1];
         }
-        if (lane == 0) {
+        const bool lng = a1 - a0 > ROW_STATS_LONG;
+        long long w = 0;
+        int mb = 0;
+        if (!lng) row_stats_entries<4>(A, B, a0 + sl, a1, 8, w, mb);
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            w += __shfl_xor_sync(FULL, w, o);
+            mb = max(mb, __shfl_xor_sync(FULL, mb, o));
+        }
+        if (sl == 0 && r < A.m && !lng) {
             work[r] = w;
             maxb[r] = mb;
+        }
+        // the step's long rows, one at a time with all 32 lanes
+        for (unsigned lm = __ballot_sync(FULL, lng && sl == 0); lm; lm &= lm - 1) {
+            const int g = (__ffs(lm) - 1) >> 3;
+            const int64_t rr = base + g;
+            const int64_t b0 = __shfl_sync(FULL, a0, 8 * g), b1 = __shfl_sync(FULL, a1, 8 * g);
+            long long lw = 0;
+            int lmb = 0;
+            row_stats_entries<8>(A, B, b0 + lane, b1, 32, lw, lmb);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lw += __shfl_xor_sync(FULL, lw, o);
+                lmb = max(lmb, __shfl_xor_sync(FULL, lmb, o));
+            }
+            if (lane == 0) {
+                work[rr] = lw;
+                maxb[rr] = lmb;
+            }
         }
     }
 }

@@ -122,3 +122,21 @@ def test_learned_choices_match_numpy_inference(gk, cuda):
         # ties within float round-off may resolve either way
         if abs(np.sort(scores)[1] - scores.min()) > 1e-4 if len(cand) > 1 else True:
             assert learned[b] == best, (b, learned[b], best)
+
+
+@pytest.mark.parametrize("maker", [lambda gk: gk.gen_rmat(16, 16, seed=9), lambda gk: gk.gen_er(30000, 400000, seed=9)])
+def test_bin_statistics_match_numpy(gk, cuda, maker):
+    """The row statistics behind the bins (work = the B-row lengths streamed
+    by a row, max_b = its longest B row) summed over the bins equal a numpy
+    recount, on a graph with hub rows (longer than the 256 entries that move
+    a row from eight lanes to a whole warp) and on one without."""
+    from graphkokkos_b200 import sched
+    A = maker(gk)
+    L = gk.lower_host(A)
+    rp = np.asarray(L.rowptr, dtype=np.int64)
+    col = np.asarray(L.col)[:L.nnz].astype(np.int64)
+    ln = np.diff(rp)
+    work = np.add.reduceat(ln[col], rp[:-1][ln > 0]) if L.nnz else np.zeros(0)
+    stats, _, _ = sched.bins(L.to("cuda"), 0)
+    assert int(stats[:, 3].sum()) == int(work.sum())
+    assert int(stats[:, 4].max()) == int(ln[col].max())
