@@ -18,9 +18,10 @@
 //    lanes: each lane computes its entry's pair count, a warp scan gives the
 //    offsets, and every lane takes pairs lane, lane+32, ... locating the pair's
 //    A entry by a five-step search over the scan held in the lanes' registers
-//    (shuffles).  No lane idles on an A entry with few pairs.  A lane runs two
-//    pairs' binary searches interleaved (two dependent-load chains in flight:
-//    the kernel is bound by the latency of those loads).
+//    (shuffles).  No lane idles on an A entry with few pairs.  A lane runs
+//    several pairs' binary searches interleaved (three dependent-load chains
+//    in flight for a warp per row, two for the smaller groups: the kernel is
+//    bound by the latency of those loads).
 //  * Mask rows longer than CAP are taken in chunks of CAP columns; a pair is
 //    seen in exactly one chunk, so chunking adds no lookups.
 //  * Integer terms are summed exactly as in the other kinds (32-bit wrapping
@@ -29,6 +30,25 @@
 //    take two and four short rows at a time (variants 22 and 23, the small
 //    rows of a many-graph batch), every collective confined to the group.
 #pragma once
+
+// Pairs whose binary searches a lane runs interleaved, and the resident
+// 256-thread CTAs per SM its register cap aims at: a warp per row (variant 17)
+// runs three chains at five CTAs (RMAT-24: 54.4 -> 52.5 ms against two at six,
+// four at four 55.3 ms); half- and quarter-warp groups keep two chains and get
+// four CTAs, whose 64 registers hold their per-group state without spills
+// (4,096-graph batch, variant 23: 46.5 -> 42.4 ms against five CTAs).
+#ifndef GK_SEARCH_PAIRS
+#define GK_SEARCH_PAIRS 3
+#endif
+#ifndef GK_SEARCH_PAIRS_SUB
+#define GK_SEARCH_PAIRS_SUB 2
+#endif
+#ifndef GK_SEARCH_MINB
+#define GK_SEARCH_MINB 5
+#endif
+#ifndef GK_SEARCH_MINB_SUB
+#define GK_SEARCH_MINB_SUB 4
+#endif
 
 // First index q in [0, n) of the sorted shared-memory array k with k[q] >= x
 // (strict = false) or k[q] > x (strict = true); n when there is none.
@@ -66,12 +86,13 @@ struct Pair {
 };
 
 // G lanes per row (G = 32: a warp; 16 and 8: two and four short rows per
-// warp), CAP mask columns per chunk in shared memory.
-// Sub-warp groups hold more per-lane state (group masks, shuffle widths):
-// they are register-capped for five CTAs per SM instead of six.
+// warp), CAP mask columns per chunk in shared memory.  Sub-warp groups hold
+// more per-lane state (group masks, shuffle widths).
 template <int NT, int G, int CAP, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_THREADS / NT) k_search(KArgs p) {
+__global__ void __launch_bounds__(NT, G < 32 ? GK_SEARCH_MINB_SUB : GK_SEARCH_MINB) k_search(KArgs p) {
+    static_assert(NT == 256, "the register caps assume 256-thread CTAs");
     constexpr bool ACC = (EPI == EPI_WRITE);
+    constexpr int NP = G < 32 ? GK_SEARCH_PAIRS_SUB : GK_SEARCH_PAIRS;
     constexpr int NG = NT / G;
     const unsigned gmask = group_mask<G>();
     extern __shared__ int smem[];
@@ -134,13 +155,13 @@ __global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_
                 }
                 const int total = __shfl_sync(gmask, incl, G - 1, G);
                 const int excl = incl - n;
-                // two pairs per lane per round (pairs pb + lane and
-                // pb + G + lane), their binary searches interleaved so that
-                // two dependent-load chains are in flight per lane
-                for (int pb = 0; pb < total; pb += 2 * G) {
-                    Pair P[2];
+                // NP pairs per lane per round (pairs pb + lane, pb + G +
+                // lane, ...), their binary searches interleaved so that NP
+                // dependent-load chains are in flight per lane
+                for (int pb = 0; pb < total; pb += NP * G) {
+                    Pair P[NP];
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
+                    for (int h = 0; h < NP; ++h) {
                         const int pp = pb + G * h + lane;
                         // the pair's A entry: the first lane j whose inclusive
                         // count exceeds pp (binary lifting over the lanes)
@@ -164,13 +185,17 @@ __global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_
                     }
                     // last position with B.col <= c in each pair's B row
                     // (row[0] <= c holds: c lies inside the row's range)
-                    while (P[0].len > 1 || P[1].len > 1) {
-                        int x[2];
+                    while (true) {
+                        bool more = false;
 #pragma unroll
-                        for (int h = 0; h < 2; ++h)
+                        for (int h = 0; h < NP; ++h) more |= P[h].len > 1;
+                        if (!more) break;
+                        int x[NP];
+#pragma unroll
+                        for (int h = 0; h < NP; ++h)
                             if (P[h].len > 1) x[h] = __ldg(P[h].row + P[h].lo + (P[h].len >> 1));
 #pragma unroll
-                        for (int h = 0; h < 2; ++h)
+                        for (int h = 0; h < NP; ++h)
                             if (P[h].len > 1) {
                                 const int half = P[h].len >> 1;
                                 if (x[h] <= P[h].c) P[h].lo += half;
@@ -178,7 +203,7 @@ __global__ void __launch_bounds__(NT, G < 32 ? (GK_LB_THREADS / NT) - 1 : GK_LB_
                             }
                     }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
+                    for (int h = 0; h < NP; ++h) {
                         if (P[h].live && __ldg(P[h].row + P[h].lo) == P[h].c) {
                             const uint32_t w =
                                 (VAL && p.B.val)
