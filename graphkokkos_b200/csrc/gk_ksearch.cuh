@@ -36,7 +36,10 @@
 // runs three chains at five CTAs (RMAT-24: 54.4 -> 52.5 ms against two at six,
 // four at four 55.3 ms); half- and quarter-warp groups keep two chains and get
 // four CTAs, whose 64 registers hold their per-group state without spills
-// (4,096-graph batch, variant 23: 46.5 -> 42.4 ms against five CTAs).
+// (4,096-graph batch, variant 23: 46.5 -> 42.4 ms against five CTAs).  With
+// values written (k-truss support) the warp shape keeps two chains at six
+// CTAs: its accumulator updates need the registers (three chains at five CTAs
+// spilled and took variant 17's k-truss passes from 6.9 to 8.2 ms).
 #ifndef GK_SEARCH_PAIRS
 #define GK_SEARCH_PAIRS 3
 #endif
@@ -48,6 +51,9 @@
 #endif
 #ifndef GK_SEARCH_MINB_SUB
 #define GK_SEARCH_MINB_SUB 4
+#endif
+#ifndef GK_SEARCH_MINB_WRITE
+#define GK_SEARCH_MINB_WRITE 6
 #endif
 
 // First index q in [0, n) of the sorted shared-memory array k with k[q] >= x
@@ -89,10 +95,12 @@ struct Pair {
 // warp), CAP mask columns per chunk in shared memory.  Sub-warp groups hold
 // more per-lane state (group masks, shuffle widths).
 template <int NT, int G, int CAP, int EPI, bool VAL>
-__global__ void __launch_bounds__(NT, G < 32 ? GK_SEARCH_MINB_SUB : GK_SEARCH_MINB) k_search(KArgs p) {
+__global__ void __launch_bounds__(NT, G < 32 ? GK_SEARCH_MINB_SUB
+                                             : (EPI == EPI_WRITE ? GK_SEARCH_MINB_WRITE : GK_SEARCH_MINB))
+    k_search(KArgs p) {
     static_assert(NT == 256, "the register caps assume 256-thread CTAs");
     constexpr bool ACC = (EPI == EPI_WRITE);
-    constexpr int NP = G < 32 ? GK_SEARCH_PAIRS_SUB : GK_SEARCH_PAIRS;
+    constexpr int NP = (G < 32 || ACC) ? GK_SEARCH_PAIRS_SUB : GK_SEARCH_PAIRS;
     constexpr int NG = NT / G;
     const unsigned gmask = group_mask<G>();
     extern __shared__ int smem[];
