@@ -7,7 +7,9 @@
 // OpenMP thread with a dense accumulator of B.n entries per thread.
 //
 // B200 design (all device-side, no host synchronisation, graph-capturable):
-//  1. k_row_stats   one warp per row: work_i = sum_{k in A_i} nnz(B_k), max nnz(B_k)
+//  1. k_row_stats   eight lanes per row (a warp for long rows): work_i = sum over
+//                   k in A_i of nnz(B_k), and the largest nnz(B_k), from B's row
+//                   lengths as 32-bit words (k_row_lengths)
 //  2. k_bin_rows    bin each row by (log2 nnz(M_i), log2 mean nnz(B_k)); per-bin stats
 //  3. sched_choose  one variant per bin (plain heuristic or learned MLP)
 //  4. k_count/k_scatter  counting sort of the rows by variant; block kinds also
@@ -71,12 +73,21 @@ struct KArgs {
 // that a hub row (10^5 entries) is one warp's loop.
 constexpr int ROW_STATS_LONG = 256;
 
+// B's row lengths as 32-bit words: the row statistics gather one per A entry
+// at random, and 4 bytes a row stay in L2 where B's 8-byte row pointers (two
+// per lookup, 134 MB at 2^24 rows) do not.
+__global__ void k_row_lengths(DevCsr B, int32_t *blen) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < B.m; k += stride)
+        blen[k] = static_cast<int32_t>(B.rp[k + 1] - B.rp[k]);
+}
+
 // Entries t, t + step, ... < a1 of a row, U of them per lane in flight at a
-// time: the U column loads, then the U row-pointer pairs they name, so that a
-// row of at most step * U entries costs one dependent load chain.
+// time: the U column loads, then the U row lengths they name, so that a row of
+// at most step * U entries costs one dependent load chain.
 template <int U>
-__device__ __forceinline__ void row_stats_entries(const DevCsr &A, const DevCsr &B, int64_t t, int64_t a1, int step,
-                                                  long long &w, int &mb) {
+__device__ __forceinline__ void row_stats_entries(const DevCsr &A, const int32_t *__restrict__ blen, int64_t t,
+                                                  int64_t a1, int step, long long &w, int &mb) {
     for (; t < a1; t += static_cast<int64_t>(step) * U) {
         int k[U];
 #pragma unroll
@@ -84,22 +95,18 @@ __device__ __forceinline__ void row_stats_entries(const DevCsr &A, const DevCsr 
             const int64_t q = t + static_cast<int64_t>(step) * u;
             k[u] = q < a1 ? __ldg(A.col + q) : -1;
         }
-        int64_t b0[U], b1[U];
+        int len[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) len[u] = k[u] >= 0 ? __ldg(blen + k[u]) : 0;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            b0[u] = k[u] >= 0 ? __ldg(B.rp + k[u]) : 0;
-            b1[u] = k[u] >= 0 ? __ldg(B.rp + k[u] + 1) : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int len = static_cast<int>(b1[u] - b0[u]);
-            w += len;
-            mb = max(mb, len);
+            w += len[u];
+            mb = max(mb, len[u]);
         }
     }
 }
 
-__global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
+__global__ void k_row_stats(DevCsr A, const int32_t *__restrict__ blen, int64_t *work, int32_t *maxb) {
     constexpr unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, sl = lane & 7;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -113,7 +120,7 @@ __global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
         const bool lng = a1 - a0 > ROW_STATS_LONG;
         long long w = 0;
         int mb = 0;
-        if (!lng) row_stats_entries<4>(A, B, a0 + sl, a1, 8, w, mb);
+        if (!lng) row_stats_entries<4>(A, blen, a0 + sl, a1, 8, w, mb);
 #pragma unroll
         for (int o = 4; o > 0; o >>= 1) {
             w += __shfl_xor_sync(FULL, w, o);
@@ -130,7 +137,7 @@ __global__ void k_row_stats(DevCsr A, DevCsr B, int64_t *work, int32_t *maxb) {
             const int64_t b0 = __shfl_sync(FULL, a0, 8 * g), b1 = __shfl_sync(FULL, a1, 8 * g);
             long long lw = 0;
             int lmb = 0;
-            row_stats_entries<8>(A, B, b0 + lane, b1, 32, lw, lmb);
+            row_stats_entries<8>(A, blen, b0 + lane, b1, 32, lw, lmb);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 lw += __shfl_xor_sync(FULL, lw, o);
@@ -901,7 +908,13 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     GK_CUDA(cudaMemsetAsync(item_n, 0, sizeof(int64_t) * (m + 1), s));
 
     const int sms = c.num_sms;
-    k_row_stats<<<sms * 8, 256, 0, s>>>(A, B, work, maxb);
+    // B's row lengths live in item_ex until the item scan overwrites it (after
+    // the row statistics, in stream order); a B with more rows than that holds
+    // gets its own buffer (fixed-scratch callers are square and never do)
+    int32_t *blen = reinterpret_cast<int32_t *>(item_ex);
+    if (B.m > 2 * (m + 1)) GK_CHECK(scr.alloc(&blen, B.m));
+    k_row_lengths<<<sms * 8, 256, 0, s>>>(B, blen);
+    k_row_stats<<<sms * 8, 256, 0, s>>>(A, blen, work, maxb);
     GK_CUDA(cudaGetLastError());
     k_bin_rows<<<sms * 2, 256, 0, s>>>(A, M, work, maxb, bin, bins);
     GK_CUDA(cudaGetLastError());
@@ -915,7 +928,7 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     if (rq.variant_of_bin_out && rq.force_variant < 0)
         GK_CUDA(cudaMemcpyAsync(rq.variant_of_bin_out, var_of_bin, sizeof(int) * NBINS, cudaMemcpyDeviceToDevice, s));
     if (rq.stats_only) {
-        note_launches(2);
+        note_launches(3);
         return GK_OK;
     }
     k_count_rows<<<sms * 2, 256, 0, s>>>(A, M, work, bin, var_of_bin, rq.force_variant, write, vcount, vsimple);
@@ -931,7 +944,7 @@ int run_spgemm(const SpgemmRequest &rq, Scratch &scr) {
     GK_CHECK(scr.alloc(reinterpret_cast<char **>(&tmp), tmp_bytes));
     GK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, item_n, item_ex, m + 1, s));
 
-    note_launches(5);
+    note_launches(6);
 
     KArgs args;
     args.A = A;
