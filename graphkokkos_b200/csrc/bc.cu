@@ -262,28 +262,29 @@ __device__ int bc_plain_shape(const BcState *st, int64_t m, int64_t nnz, int W) 
 // decides.
 __global__ void k_bc_choose(BcState *st, int force, int sched, int64_t m, int64_t nnz, int W, float *feat_log,
                             int log_cap) {
+    // one warp: the model's hidden units one per lane (mlp_forward_warp2)
     __shared__ float sw[MLP_SIZE];
     const bool learned = force < 0 && sched == GK_SCHED_LEARNED;
-    if (learned) {
-        for (int i = threadIdx.x; i < MLP_SIZE; i += blockDim.x) sw[i] = d_mlp_bc[i];
-        __syncwarp();
-    }
-    if (threadIdx.x != 0) return;
+    const int lane = threadIdx.x & 31;
     float f[BC_FEAT];
     bc_features(st, m, nnz, W, f);
     int mode;
     if (force >= 0) {
         mode = force;
-    } else if (sched == GK_SCHED_LEARNED) {
+    } else if (learned) {
+        for (int i = lane; i < MLP_SIZE; i += 32) sw[i] = d_mlp_bc[i];
+        __syncwarp();
         // the plain rule's shape unless the model predicts the other one at
         // least 10% faster (the row-bin scheduler's margin)
-        float x[NFEAT], h1[MLP_H], h2[MLP_H], out[NV];
-        mlp_forward(sw, f, x, h1, h2, out);
+        float o[2];
+        mlp_forward_warp2(sw, f, &o[0], &o[1]);
         const int plain = bc_plain_shape(st, m, nnz, W);
-        mode = out[plain] - out[1 - plain] >= 0.1375f ? 1 - plain : plain;
+        mode = o[plain] - o[1 - plain] >= 0.1375f ? 1 - plain : plain;
     } else {
         mode = bc_plain_shape(st, m, nnz, W);
     }
+    __syncwarp();  // every lane has read the state before lane 0 updates it
+    if (lane != 0) return;
     st->mode = mode;
     if (mode == BC_PUSH) ++st->pushes;
     else ++st->pulls;
@@ -851,6 +852,37 @@ __global__ void k_bc_bwd_end(BcState *st, cudaGraphConditionalHandle h, int in_g
     if (in_graph) cudaGraphSetConditional(h, st->bd >= 1 ? 1u : 0u);
 }
 
+// Row index of every entry (a warp per row), for the per-entry check below.
+__global__ void k_bc_entry_rows(DevCsr A, int32_t *row) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.m; i += warps)
+        for (int64_t p = A.rp[i] + lane; p < A.rp[i + 1]; p += 32) row[p] = static_cast<int32_t>(i);
+}
+
+// *asym = 1 unless every row is strictly increasing and every entry (i, j)
+// has its mirror (j, i): then the pattern equals its transpose entry for
+// entry (sorted rows, no duplicates).  A thread per entry, one binary search
+// of i in row j (a warp per row would serialise on a hub's searches).
+__global__ void k_bc_mirror_check(DevCsr A, const int32_t *row, int *asym) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < A.nnz; p += stride) {
+        const int i = row[p], j = A.col[p];
+        if (p + 1 < A.rp[i + 1] && A.col[p + 1] <= j) {
+            atomicExch(asym, 1);
+            continue;
+        }
+        int64_t lo = A.rp[j], hi = A.rp[j + 1];
+        const int64_t end = hi;
+        while (lo < hi) {
+            const int64_t md = (lo + hi) >> 1;
+            if (A.col[md] < i) lo = md + 1;
+            else hi = md;
+        }
+        if (lo == end || A.col[lo] != i) atomicExch(asym, 1);
+    }
+}
+
 __global__ void k_heavy_list(DevCsr A, int32_t *list, int *count) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.m; i += stride)
@@ -1239,15 +1271,40 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const B
     const int sms = ctx().num_sms;
     BcBuffers g;
     g.A = A;
-    int64_t *trp;
-    int32_t *tcol, *tval = nullptr;
-    GK_CHECK(scr.alloc(&trp, A.m + 1));
-    GK_CHECK(scr.alloc(&tcol, A.nnz > 0 ? A.nnz : 1));
-    if (A.val) GK_CHECK(scr.alloc(&tval, A.nnz > 0 ? A.nnz : 1));
-    GK_CHECK(transpose_device(A, trp, tcol, tval, s, scr));
-    g.AT = DevCsr{A.m, A.m, A.nnz, trp, tcol, tval};
+    // The pull shapes read A's transpose.  A pattern (no values) with sorted
+    // rows that equals its transpose (an undirected graph) is its own: the
+    // radix-sort transpose and the second heavy-vertex set are then skipped.
+    bool self_transpose = false;
+    if (!A.val && A.nnz > 0) {
+        Scratch cs(s);
+        int32_t *row;
+        int *asym;
+        GK_CHECK(cs.alloc(&row, A.nnz));
+        GK_CHECK(cs.alloc(&asym, 1));
+        GK_CUDA(cudaMemsetAsync(asym, 0, sizeof(int), s));
+        k_bc_entry_rows<<<sms * 8, 256, 0, s>>>(A, row);
+        k_bc_mirror_check<<<sms * 8, 256, 0, s>>>(A, row, asym);
+        note_launches(2);
+        GK_CUDA(cudaGetLastError());
+        int h_asym = 1;
+        GK_CUDA(cudaMemcpyAsync(&h_asym, asym, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GK_CUDA(cudaStreamSynchronize(s));
+        self_transpose = h_asym == 0;
+    }
+    if (self_transpose) {
+        g.AT = A;
+    } else {
+        int64_t *trp;
+        int32_t *tcol, *tval = nullptr;
+        GK_CHECK(scr.alloc(&trp, A.m + 1));
+        GK_CHECK(scr.alloc(&tcol, A.nnz > 0 ? A.nnz : 1));
+        if (A.val) GK_CHECK(scr.alloc(&tval, A.nnz > 0 ? A.nnz : 1));
+        GK_CHECK(transpose_device(A, trp, tcol, tval, s, scr));
+        g.AT = DevCsr{A.m, A.m, A.nnz, trp, tcol, tval};
+    }
     GK_CHECK(heavy_set(g.A, &g.hA, s, scr));
-    GK_CHECK(heavy_set(g.AT, &g.hAT, s, scr));
+    if (self_transpose) g.hAT = g.hA;
+    else GK_CHECK(heavy_set(g.AT, &g.hAT, s, scr));
     GK_CUDA(cudaMemsetAsync(bc, 0, sizeof(double) * A.m, s));
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);

@@ -160,6 +160,8 @@ constexpr int MLP_SIZE = MLP_H * NFEAT + MLP_H + MLP_H * MLP_H + MLP_H + NV * ML
 // Forward pass of the network (mlp.cu): out[NV] from the raw features f;
 // x, h1, h2 are caller scratch of NFEAT, MLP_H, MLP_H floats.
 __device__ void mlp_forward(const float *w, const float *f, float *x, float *h1, float *h2, float *out);
+// outputs 0 and 1 of the same network, computed by one full warp (mlp.cu)
+__device__ void mlp_forward_warp2(const float *w, const float *f, float *o0, float *o1);
 #endif
 
 }  // namespace gk

@@ -53,6 +53,32 @@ __device__ void mlp_forward(const float *w, const float *f, float *x, float *h1,
     }
 }
 
+// The same network for one warp, outputs 0 and 1 only (the BC level shapes):
+// lane j computes hidden unit j of each layer; every sum runs in the order of
+// mlp_forward's (inputs of a unit in index order, each gathered from its lane),
+// so the outputs are the same floats.  Call with all 32 lanes.
+__device__ void mlp_forward_warp2(const float *w, const float *f, float *o0, float *o1) {
+    static_assert(MLP_H == 32, "one hidden unit per lane");
+    const int j = threadIdx.x & 31;
+    float x[NFEAT];
+#pragma unroll
+    for (int i = 0; i < NFEAT; ++i) x[i] = (f[i] - w[P_MU + i]) / w[P_SG + i];
+    float a = w[P_B1 + j];
+#pragma unroll
+    for (int i = 0; i < NFEAT; ++i) a += w[P_W1 + j * NFEAT + i] * x[i];
+    const float h1 = a > 0.f ? a : 0.f;
+    a = w[P_B2 + j];
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; ++i) a += w[P_W2 + j * MLP_H + i] * __shfl_sync(0xFFFFFFFFu, h1, i);
+    const float h2 = a > 0.f ? a : 0.f;
+    const int v = j < 2 ? j : 0;
+    a = w[P_B3 + v];
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; ++i) a += w[P_W3 + v * MLP_H + i] * __shfl_sync(0xFFFFFFFFu, h2, i);
+    *o0 = __shfl_sync(0xFFFFFFFFu, a, 0);
+    *o1 = __shfl_sync(0xFFFFFFFFu, a, 1);
+}
+
 // Adds d(loss)/d(params) of one sample into g (shared memory, atomics) and
 // returns the sample's squared-error sum.  scale = 1 / (number of measured pairs).
 __device__ float mlp_backward(const float *w, const float *f, const float *y, const float *mask, float scale,
