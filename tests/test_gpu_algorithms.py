@@ -129,6 +129,24 @@ def test_bc_closed_forms_and_host_buffers(gk, cuda):
     assert bc[0] == pytest.approx(30.0) and np.all(bc[1:] == 0)
 
 
+def test_bc_transpose_paths(gk, orc, cuda):
+    """An undirected pattern with sorted rows is used as its own transpose; the
+    same graph with each row's columns reversed (unsorted) or with unit values
+    goes through the radix-sort transpose.  All three give the oracle's scores."""
+    import torch
+    A = gk.gen_rmat(11, 16, seed=13)
+    src = np.random.default_rng(13).choice(A.m, size=96, replace=False)
+    want = orc.bc_f64(A, src)
+    rp = np.asarray(A.rowptr, dtype=np.int64)
+    col = np.asarray(A.col)[:A.nnz]
+    rev = np.concatenate([col[rp[i]:rp[i + 1]][::-1] for i in range(A.m)]).astype(np.int32)
+    unsorted = gk.Csr(A.m, A.n, torch.from_numpy(rp.copy()), torch.from_numpy(rev), None, A.nnz)
+    valued = gk.Csr(A.m, A.n, torch.from_numpy(rp.copy()), torch.from_numpy(col.astype(np.int32)),
+                    torch.ones(A.nnz, dtype=torch.int32), A.nnz)
+    for X in (A, unsorted, valued):
+        G.assert_bc_close(gk.bc_batch(dev(X), src).cpu().numpy(), want, BC_RTOL)
+
+
 def test_bc_directed(gk, orc, cuda):
     A = G.random_csr(300, 300, 0.02, seed=11)
     src = np.arange(0, 300, 7)
