@@ -860,18 +860,23 @@ __global__ void k_bc_entry_rows(DevCsr A, int32_t *row) {
         for (int64_t p = A.rp[i] + lane; p < A.rp[i + 1]; p += 32) row[p] = static_cast<int32_t>(i);
 }
 
-// *asym = 1 unless every row is strictly increasing and every entry (i, j)
-// has its mirror (j, i): then the pattern equals its transpose entry for
-// entry (sorted rows, no duplicates).  A thread per entry, one binary search
-// of i in row j (a warp per row would serialise on a hub's searches).
-__global__ void k_bc_mirror_check(DevCsr A, const int32_t *row, int *asym) {
+// Symmetry of a pattern with sorted rows.  out[0] = 1 when a row is not
+// strictly increasing or an entry (i, j > i) has no mirror (j, i); out[1] and
+// out[2] count the entries above and below the diagonal.  Every upper entry
+// having its mirror maps the upper entries one to one onto lower ones (no
+// duplicates), so equal counts mean that the pattern equals its transpose
+// entry for entry; only the upper half is searched.  A thread per entry, one
+// binary search of i in row j (a warp per row would serialise on a hub's).
+__global__ void k_bc_mirror_check(DevCsr A, const int32_t *row, unsigned long long *out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned up = 0, lo_cnt = 0;
+    bool bad = false;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < A.nnz; p += stride) {
         const int i = row[p], j = A.col[p];
-        if (p + 1 < A.rp[i + 1] && A.col[p + 1] <= j) {
-            atomicExch(asym, 1);
-            continue;
-        }
+        if (p + 1 < A.rp[i + 1] && A.col[p + 1] <= j) bad = true;
+        if (j < i) ++lo_cnt;
+        if (j <= i) continue;
+        ++up;
         int64_t lo = A.rp[j], hi = A.rp[j + 1];
         const int64_t end = hi;
         while (lo < hi) {
@@ -879,7 +884,14 @@ __global__ void k_bc_mirror_check(DevCsr A, const int32_t *row, int *asym) {
             if (A.col[md] < i) lo = md + 1;
             else hi = md;
         }
-        if (lo == end || A.col[lo] != i) atomicExch(asym, 1);
+        if (lo == end || A.col[lo] != i) bad = true;
+    }
+    if (bad) atomicExch(out, 1ull);
+    up = __reduce_add_sync(0xFFFFFFFFu, up);
+    lo_cnt = __reduce_add_sync(0xFFFFFFFFu, lo_cnt);
+    if ((threadIdx.x & 31) == 0) {
+        if (up) atomicAdd(out + 1, static_cast<unsigned long long>(up));
+        if (lo_cnt) atomicAdd(out + 2, static_cast<unsigned long long>(lo_cnt));
     }
 }
 
@@ -1278,18 +1290,18 @@ int bc_device(const DevCsr &A, const int32_t *src, int nsrc, double *bc, const B
     if (!A.val && A.nnz > 0) {
         Scratch cs(s);
         int32_t *row;
-        int *asym;
+        unsigned long long *chk;
         GK_CHECK(cs.alloc(&row, A.nnz));
-        GK_CHECK(cs.alloc(&asym, 1));
-        GK_CUDA(cudaMemsetAsync(asym, 0, sizeof(int), s));
+        GK_CHECK(cs.alloc(&chk, 3));
+        GK_CUDA(cudaMemsetAsync(chk, 0, 3 * sizeof(unsigned long long), s));
         k_bc_entry_rows<<<sms * 8, 256, 0, s>>>(A, row);
-        k_bc_mirror_check<<<sms * 8, 256, 0, s>>>(A, row, asym);
+        k_bc_mirror_check<<<sms * 8, 256, 0, s>>>(A, row, chk);
         note_launches(2);
         GK_CUDA(cudaGetLastError());
-        int h_asym = 1;
-        GK_CUDA(cudaMemcpyAsync(&h_asym, asym, sizeof(int), cudaMemcpyDeviceToHost, s));
+        unsigned long long h[3] = {1, 0, 0};
+        GK_CUDA(cudaMemcpyAsync(h, chk, sizeof(h), cudaMemcpyDeviceToHost, s));
         GK_CUDA(cudaStreamSynchronize(s));
-        self_transpose = h_asym == 0;
+        self_transpose = h[0] == 0 && h[1] == h[2];
     }
     if (self_transpose) {
         g.AT = A;
